@@ -1,0 +1,195 @@
+"""ctypes bindings of the in-tree native libraries (bin/libkdtree.so,
+bin/libcoords.so).
+
+The structure layouts are the reference's C ABI (src/kdtree.h:11-41).  Unlike
+the reference's ctypes declaration (corruscant/clustering.py:36-45, where
+``args`` is a single pointer and the struct is 48 bytes), ``KdTree`` declares
+``args`` as three pointers, so it is the full 64-byte ``kdtree_t`` that
+``tree_construct`` returns by value.
+
+There is no fallback: if the library is missing or cannot find a CUDA device,
+calls raise ``NativeError``.
+"""
+import ctypes
+import os
+from ctypes import POINTER, Structure, c_char_p, c_double, c_int, c_longlong, c_uint, c_void_p
+
+import numpy as np
+
+PROJECT_PATH = os.path.dirname(os.path.abspath(__file__))
+BIN = os.path.join(PROJECT_PATH, "bin")
+
+KD_MODE_MIXED = 0
+KD_MODE_FP64 = 1
+
+
+class NativeError(RuntimeError):
+    """An error reported by the native library (code and message)."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Datum(Structure):
+    _fields_ = [("value", c_double * 3), ("field", c_uint, 8), ("weight", c_uint, 8)]
+
+
+class Node(Structure):
+    _fields_ = [("data", Datum), ("has_lchild", c_uint, 1), ("has_rchild", c_uint, 1),
+                ("dim", c_uint, 8)]
+
+
+class KdTree(Structure):
+    _fields_ = [("node_data", POINTER(Node)), ("size", c_int), ("memsize", c_int),
+                ("num_fields", c_int), ("data", POINTER(Datum)), ("fields", POINTER(c_int)),
+                ("args", POINTER(c_int) * 3)]
+
+
+class CountStats(Structure):
+    _fields_ = [("pairs_tested", c_longlong), ("pairs_rechecked", c_longlong),
+                ("pairs_accepted", c_longlong), ("pairs_wide", c_longlong),
+                ("edge_pairs", c_longlong), ("warp_tiles", c_longlong), ("entries", c_longlong), ("ms_traverse", c_double), ("ms_tiles", c_double),
+                ("ms_total", c_double), ("tile_launches", c_int), ("launches", c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+assert ctypes.sizeof(KdTree) == 64
+assert ctypes.sizeof(Node) == 40
+
+_KD = None
+
+
+def loadlib(name):
+    """Load ``bin/<name>.so`` (the in-tree build)."""
+    path = os.path.join(BIN, name + ".so")
+    if not os.path.exists(path):
+        raise OSError(f"{path} not found: build it with "
+                      f"`python -c 'import __graft_entry__; __graft_entry__.build()'` "
+                      f"or `make -C corruscant_b200/csrc`")
+    return ctypes.CDLL(path)
+
+
+def kdlib():
+    global _KD
+    if _KD is None:
+        L = loadlib("libkdtree")
+        L.tree_construct.restype = KdTree
+        L.tree_construct.argtypes = [POINTER(c_double), POINTER(c_int), c_int, c_int]
+        L.pair_count.restype = POINTER(c_longlong)
+        L.pair_count.argtypes = [KdTree, POINTER(c_double), POINTER(c_int), c_int, c_int,
+                                 c_double, c_int]
+        L.destroy.restype = None
+        L.destroy.argtypes = [KdTree]
+        L.kd_last_error.restype = c_int
+        L.kd_last_error.argtypes = [c_char_p, c_int]
+        L.kd_free_counts.restype = None
+        L.kd_free_counts.argtypes = [c_void_p]
+        L.kd_count_radii.restype = c_int
+        L.kd_count_radii.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int,
+                                     POINTER(c_longlong), POINTER(CountStats)]
+        L.kd_count_points.restype = c_int
+        L.kd_count_points.argtypes = [KdTree, POINTER(c_double), POINTER(c_int), c_int, c_int,
+                                      POINTER(c_double), c_int, c_int, POINTER(c_longlong),
+                                      POINTER(CountStats)]
+        L.kd_tree_permutation.restype = c_int
+        L.kd_tree_permutation.argtypes = [KdTree, POINTER(c_int)]
+        L.kd_tree_input_size.restype = c_int
+        L.kd_tree_input_size.argtypes = [KdTree]
+        _KD = L
+    return _KD
+
+
+def last_error():
+    buf = ctypes.create_string_buffer(256)
+    code = kdlib().kd_last_error(buf, 256)
+    return code, buf.value.decode(errors="replace")
+
+
+def raise_last(default="native call failed"):
+    code, msg = last_error()
+    raise NativeError(code or -1, msg or default)
+
+
+def dptr(a):
+    return a.ctypes.data_as(POINTER(c_double))
+
+
+def iptr(a):
+    return None if a is None else a.ctypes.data_as(POINTER(c_int))
+
+
+def build_tree(points, fields, num_fields):
+    """tree_construct on C-contiguous float64 (N,3) points and int32 fields."""
+    t = kdlib().tree_construct(dptr(points), iptr(fields), c_int(points.shape[0]),
+                               c_int(num_fields))
+    if not t.node_data:
+        raise_last("tree_construct failed")
+    return t
+
+
+def node_fields(t):
+    """Semantic node fields of a kdtree_t as numpy arrays (length memsize)."""
+    m = t.memsize
+    raw = np.ctypeslib.as_array(ctypes.cast(t.node_data, POINTER(ctypes.c_uint8)),
+                                shape=(m * 40,)).reshape(m, 40)
+    xyz = raw[:, :24].copy().view(np.float64).reshape(m, 3)
+    fw = raw[:, 24:28].copy().view(np.uint32).ravel().astype(np.int64)
+    fl = raw[:, 32:36].copy().view(np.uint32).ravel().astype(np.int64)
+    return dict(xyz=xyz, field=(fw & 0xFF).astype(np.int32),
+                weight=((fw >> 8) & 0xFF).astype(np.int32),
+                has_l=(fl & 1).astype(np.int32), has_r=((fl >> 1) & 1).astype(np.int32),
+                dim=((fl >> 2) & 0xFF).astype(np.int32))
+
+
+def count_radii(tree, query, radii, mode=KD_MODE_MIXED, with_stats=False):
+    """Cumulative counts, shape (len(radii), Fq*Ft), for all radii in one pass."""
+    radii = np.require(np.asarray(radii, dtype=np.float64), requirements="AC")
+    out = np.zeros((len(radii), query.num_fields * tree.num_fields), dtype=np.int64)
+    st = CountStats()
+    rc = kdlib().kd_count_radii(tree, query, dptr(radii), c_int(len(radii)), c_int(mode),
+                                out.ctypes.data_as(POINTER(c_longlong)), ctypes.byref(st))
+    if rc != 0:
+        raise_last()
+    return (out, st.as_dict()) if with_stats else out
+
+
+def count_points(tree, points, fields, num_fields, radii, mode=KD_MODE_MIXED, with_stats=False):
+    points = np.require(points, dtype=np.float64, requirements="AC")
+    fields = None if fields is None else np.require(fields, dtype=np.int32, requirements="AC")
+    radii = np.require(np.asarray(radii, dtype=np.float64), requirements="AC")
+    out = np.zeros((len(radii), num_fields * tree.num_fields), dtype=np.int64)
+    st = CountStats()
+    rc = kdlib().kd_count_points(tree, dptr(points), iptr(fields), c_int(points.shape[0]),
+                                 c_int(num_fields), dptr(radii), c_int(len(radii)), c_int(mode),
+                                 out.ctypes.data_as(POINTER(c_longlong)), ctypes.byref(st))
+    if rc != 0:
+        raise_last()
+    return (out, st.as_dict()) if with_stats else out
+
+
+def pair_count(tree, points, fields, num_fields, r):
+    """The reference entry point: one radius, malloc'd result freed here."""
+    points = np.require(points, dtype=np.float64, requirements="AC")
+    fields = None if fields is None else np.require(fields, dtype=np.int32, requirements="AC")
+    L = kdlib()
+    p = L.pair_count(tree, dptr(points), iptr(fields), c_int(points.shape[0]),
+                     c_int(num_fields), c_double(r), c_int(1))
+    if not p:
+        raise_last("pair_count failed")
+    out = np.ctypeslib.as_array(p, shape=(num_fields * tree.num_fields,)).copy()
+    L.kd_free_counts(ctypes.cast(p, c_void_p))
+    return out
+
+
+def permutation(tree):
+    perm = np.zeros(tree.size, dtype=np.int32)
+    if kdlib().kd_tree_permutation(tree, iptr(perm)) != 0:
+        raise_last()
+    return perm
+
+
+def destroy(tree):
+    kdlib().destroy(tree)

@@ -1,0 +1,374 @@
+/*
+ * C host side of libkdtree.so: the reference ABI (tree_construct, pair_count,
+ * destroy) and the additive kd_* entry points, on top of the GPU catalog
+ * (kd_build.cu) and counter (kd_count.cu).
+ *
+ * Handles: tree_construct returns the reference's 64-byte kdtree_t by value
+ * (kdbuild.c:513-536).  Its node_data is a host array of node_t, as the
+ * reference returns; the device-side catalog behind it is found again from
+ * that pointer through a registry, so a kdtree_t copied by value (ctypes,
+ * C structs) keeps working.
+ */
+#define _GNU_SOURCE
+#include <math.h>
+#include <pthread.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "kd_internal.h"
+
+/* ------------------------------------------------------------------ errors */
+
+static __thread int g_code;
+static __thread char g_msg[256];
+
+void kd_set_error(int code, const char *fmt, ...)
+{
+    va_list ap;
+    g_code = code;
+    va_start(ap, fmt);
+    vsnprintf(g_msg, sizeof g_msg, fmt, ap);
+    va_end(ap);
+}
+
+int kd_last_error(char *buf, int len)
+{
+    if (buf && len > 0) {
+        strncpy(buf, g_code ? g_msg : "", (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return g_code;
+}
+
+static void clear_error(void)
+{
+    g_code = 0;
+    g_msg[0] = 0;
+}
+
+/* ---------------------------------------------------------------- registry */
+
+typedef struct kd_handle {
+    kd_catalog cat;
+    node_t *nodes;
+    struct kd_handle *next;
+} kd_handle;
+
+static pthread_mutex_t g_lock = PTHREAD_MUTEX_INITIALIZER;
+static kd_handle *g_handles;
+
+static kd_handle *lookup(const kdtree_t *t)
+{
+    kd_handle *h;
+    if (!t->node_data) return NULL;
+    pthread_mutex_lock(&g_lock);
+    for (h = g_handles; h; h = h->next)
+        if (h->nodes == t->node_data) break;
+    pthread_mutex_unlock(&g_lock);
+    return h;
+}
+
+static kd_handle *lookup_or_fail(const kdtree_t *t, const char *what)
+{
+    kd_handle *h = lookup(t);
+    if (!h) kd_set_error(KD_EINVAL, "%s: not a live tree from tree_construct", what);
+    return h;
+}
+
+/* ---------------------------------------------------------------- ABI */
+
+kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
+{
+    kdtree_t t;
+    kd_handle *h;
+    memset(&t, 0, sizeof t);
+    clear_error();
+    if (!xyz || length < 1) {
+        kd_set_error(KD_EINVAL, "tree_construct: need at least one point");
+        return t;
+    }
+    h = (kd_handle *)calloc(1, sizeof *h);
+    if (!h) {
+        kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
+        return t;
+    }
+    if (kdg_build(xyz, fields, length, num_fields, 0, &h->cat) != KD_OK) {
+        free(h);
+        return t;
+    }
+    /* calloc: empty heap slots stay zero, as in kdbuild.c:516 */
+    h->nodes = (node_t *)calloc((size_t)h->cat.memsize, sizeof(node_t));
+    if (!h->nodes || kdg_copy_nodes(&h->cat, h->nodes) != KD_OK) {
+        if (!h->nodes) kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
+        free(h->nodes);
+        kdg_free(&h->cat);
+        free(h);
+        return t;
+    }
+    kdg_drop_nodes(&h->cat);
+    pthread_mutex_lock(&g_lock);
+    h->next = g_handles;
+    g_handles = h;
+    pthread_mutex_unlock(&g_lock);
+    t.node_data = h->nodes;
+    t.size = h->cat.n_u;
+    t.memsize = h->cat.memsize;
+    t.num_fields = num_fields;
+    return t;
+}
+
+void destroy(kdtree_t t)
+{
+    kd_handle **pp, *h = NULL;
+    if (!t.node_data) return;
+    pthread_mutex_lock(&g_lock);
+    for (pp = &g_handles; *pp; pp = &(*pp)->next)
+        if ((*pp)->nodes == t.node_data) {
+            h = *pp;
+            *pp = h->next;
+            break;
+        }
+    pthread_mutex_unlock(&g_lock);
+    if (!h) return;
+    kdg_free(&h->cat);
+    free(h->nodes);
+    free(h);
+}
+
+void kd_free_counts(long long *counts) { free(counts); }
+
+int kd_tree_permutation(kdtree_t t, int *perm)
+{
+    kd_handle *h;
+    clear_error();
+    h = lookup_or_fail(&t, "kd_tree_permutation");
+    if (!h) return KD_EINVAL;
+    return kdg_copy_inorder(&h->cat, perm);
+}
+
+int kd_tree_input_size(kdtree_t t)
+{
+    kd_handle *h = lookup(&t);
+    return h ? h->cat.n_raw : -1;
+}
+
+/* ---------------------------------------------------------------- counting */
+
+static int cmp_double(const void *a, const void *b)
+{
+    double x = *(const double *)a, y = *(const double *)b;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/*
+ * Count with the tree catalog and a query catalog for all radii and write the
+ * reference's cumulative per-radius matrices, out[k][qf*Fq + tf]
+ * (kdquery.c:34: rows strided by the QUERY field count Fq).
+ */
+static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, int Fq,
+                          const double *radii, int nradii, int mode, long long *out,
+                          kd_count_stats *stats)
+{
+    double *rsq = NULL, *uniq = NULL;
+    long long *hist = NULL;
+    int k, ne = 0, rc = KD_OK;
+    size_t nrow = (size_t)Fq * (size_t)Ft;
+
+    if (mode != KD_MODE_MIXED && mode != KD_MODE_FP64) {
+        kd_set_error(KD_EINVAL, "unknown count mode %d", mode);
+        return KD_EINVAL;
+    }
+    if (Fq < 1 || Ft < 1) {
+        kd_set_error(KD_EFIELD, "field counts must be positive");
+        return KD_EFIELD;
+    }
+    if (qc->min_qf < 0) {
+        kd_set_error(KD_EFIELD, "negative query field id");
+        return KD_EFIELD;
+    }
+    /* the reference would write outside its Fq*Ft counter (kdquery.c:34) */
+    if ((long long)qc->max_qf * Fq + tc->max_tf >= (long long)nrow) {
+        kd_set_error(KD_EFIELD, "field ids overflow the %d x %d counter (qfield*%d + tfield)",
+                     Fq, Ft, Fq);
+        return KD_EFIELD;
+    }
+    for (k = 0; k < nradii; k++)
+        if (radii[k] < 0) {
+            kd_set_error(KD_ERADIUS, "negative radius %g", radii[k]);
+            return KD_ERADIUS;
+        }
+    memset(out, 0, sizeof(long long) * nrow * (size_t)nradii);
+    if (stats) memset(stats, 0, sizeof *stats);
+    rsq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
+    uniq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
+    if (!rsq || !uniq) {
+        free(rsq);
+        free(uniq);
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return KD_ENOMEM;
+    }
+    /* squared radii exactly as kdquery.c:77 forms them; NaN counts nothing */
+    for (k = 0; k < nradii; k++) rsq[k] = radii[k] * radii[k];
+    for (k = 0; k < nradii; k++)
+        if (rsq[k] == rsq[k]) uniq[ne++] = rsq[k];
+    qsort(uniq, (size_t)ne, sizeof(double), cmp_double);
+    {
+        int w = 0;
+        for (k = 0; k < ne; k++)
+            if (w == 0 || uniq[k] != uniq[w - 1]) uniq[w++] = uniq[k];
+        ne = w;
+    }
+    if (ne > KD_MAX_EDGES) {
+        kd_set_error(KD_EINVAL, "at most %d distinct radii per call", KD_MAX_EDGES);
+        rc = KD_EINVAL;
+        goto done;
+    }
+    if (ne > 0) {
+        const size_t Fqe = (size_t)qc->max_qf + 1, Fte = (size_t)tc->max_tf + 1;
+        const size_t hrow = Fqe * Fte;
+        hist = (long long *)calloc((size_t)(ne + 1) * hrow, sizeof(long long));
+        if (!hist) {
+            kd_set_error(KD_ENOMEM, "out of host memory");
+            rc = KD_ENOMEM;
+            goto done;
+        }
+        rc = kdg_count(tc, qc, uniq, ne, mode, hist, stats);
+        if (rc != KD_OK) goto done;
+        /* cumulative over sorted edges: pairs with d2 < uniq[e] */
+        for (k = 1; k < ne; k++) {
+            size_t j;
+            for (j = 0; j < hrow; j++) hist[(size_t)k * hrow + j] += hist[(size_t)(k - 1) * hrow + j];
+        }
+        for (k = 0; k < nradii; k++) {
+            int lo = 0, hi = ne;
+            size_t qf, tf;
+            long long *o = out + (size_t)k * nrow;
+            if (rsq[k] != rsq[k]) continue;
+            while (lo < hi) {
+                int m = (lo + hi) / 2;
+                if (uniq[m] < rsq[k]) lo = m + 1;
+                else hi = m;
+            }
+            for (qf = 0; qf < Fqe; qf++)
+                for (tf = 0; tf < Fte; tf++)
+                    o[qf * (size_t)Fq + tf] += hist[(size_t)lo * hrow + qf * Fte + tf];
+        }
+    }
+done:
+    free(rsq);
+    free(uniq);
+    free(hist);
+    return rc;
+}
+
+/* query catalog from raw points; NaN rows are dropped (they count nothing in
+ * the reference: every comparison with NaN is false, kdquery.c:33, :101-109) */
+static int query_catalog(const double *xyz, const int *fields, int n, int Fq, kd_catalog *qc,
+                         int *empty)
+{
+    int i, m = 0, rc;
+    double *px = NULL;
+    int *pf = NULL;
+    const double *use_x = xyz;
+    const int *use_f = fields;
+    *empty = 0;
+    for (i = 0; i < n; i++)
+        if (isnan(xyz[3 * (size_t)i]) || isnan(xyz[3 * (size_t)i + 1]) || isnan(xyz[3 * (size_t)i + 2]))
+            break;
+    if (i < n) {
+        px = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+        pf = fields ? (int *)malloc(sizeof(int) * (size_t)n) : NULL;
+        if (!px || (fields && !pf)) {
+            free(px);
+            free(pf);
+            kd_set_error(KD_ENOMEM, "out of host memory");
+            return KD_ENOMEM;
+        }
+        for (i = 0; i < n; i++) {
+            const double *p = xyz + 3 * (size_t)i;
+            if (isnan(p[0]) || isnan(p[1]) || isnan(p[2])) continue;
+            memcpy(px + 3 * (size_t)m, p, 3 * sizeof(double));
+            if (pf) pf[m] = fields[i];
+            m++;
+        }
+        use_x = px;
+        use_f = pf;
+        n = m;
+    }
+    if (n == 0) {
+        *empty = 1;
+        free(px);
+        free(pf);
+        return KD_OK;
+    }
+    rc = kdg_build(use_x, use_f, n, Fq, 1, qc);
+    free(px);
+    free(pf);
+    return rc;
+}
+
+int kd_count_points(kdtree_t tree, const double *xyz, const int *fields, int length,
+                    int num_fields, const double *radii, int nradii, int mode, long long *out,
+                    kd_count_stats *stats)
+{
+    kd_handle *h;
+    kd_catalog qc;
+    int empty = 0, rc;
+    clear_error();
+    h = lookup_or_fail(&tree, "kd_count_points");
+    if (!h) return KD_EINVAL;
+    if (length < 0 || nradii < 0 || (length > 0 && !xyz)) {
+        kd_set_error(KD_EINVAL, "kd_count_points: bad arguments");
+        return KD_EINVAL;
+    }
+    if (length == 0) {
+        memset(out, 0, sizeof(long long) * (size_t)num_fields * tree.num_fields * nradii);
+        if (stats) memset(stats, 0, sizeof *stats);
+        return KD_OK;
+    }
+    memset(&qc, 0, sizeof qc);
+    rc = query_catalog(xyz, fields, length, num_fields, &qc, &empty);
+    if (rc != KD_OK) return rc;
+    if (empty) {
+        memset(out, 0, sizeof(long long) * (size_t)num_fields * tree.num_fields * nradii);
+        if (stats) memset(stats, 0, sizeof *stats);
+        return KD_OK;
+    }
+    rc = count_catalogs(&h->cat, tree.num_fields, &qc, num_fields, radii, nradii, mode, out, stats);
+    kdg_free(&qc);
+    return rc;
+}
+
+int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradii, int mode,
+                   long long *out, kd_count_stats *stats)
+{
+    kd_handle *ht, *hq;
+    clear_error();
+    ht = lookup_or_fail(&tree, "kd_count_radii (tree)");
+    if (!ht) return KD_EINVAL;
+    hq = lookup_or_fail(&query, "kd_count_radii (query)");
+    if (!hq) return KD_EINVAL;
+    return count_catalogs(&ht->cat, tree.num_fields, &hq->cat, query.num_fields, radii, nradii,
+                          mode, out, stats);
+}
+
+long long *pair_count(kdtree_t tree, double *data, int *fields, int length, int num_fields,
+                      double r, int num_threads)
+{
+    long long *out;
+    size_t nrow = (size_t)(num_fields > 0 ? num_fields : 0) * (size_t)(tree.num_fields > 0 ? tree.num_fields : 0);
+    (void)num_threads;
+    out = (long long *)calloc(nrow ? nrow : 1, sizeof(long long));
+    if (!out) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return NULL;
+    }
+    if (kd_count_points(tree, data, fields, length, num_fields, &r, 1, KD_MODE_MIXED, out, NULL) !=
+        KD_OK) {
+        free(out);
+        return NULL;
+    }
+    return out;
+}

@@ -1,0 +1,146 @@
+/*
+ * corruscant-b200: C ABI of the GPU pair-counting library (libkdtree.so).
+ *
+ * The first part is the reference's ABI, kept binary compatible so that the
+ * reference's ctypes layer (corruscant/clustering.py:30-71) and C callers bind
+ * unchanged.  The types have the reference's field order, widths and bitfield
+ * layout (src/kdtree.h:11-41): a kdtree_t is 64 bytes, a node_t 40 bytes, and
+ * node_data is a host array of memsize nodes in heap order (root at index 1,
+ * children of p at 2p and 2p+1, empty slots all zero).
+ *
+ * The second part (kd_*) is additive: batched multi-radius counts, error
+ * reporting and resource management the reference lacks.
+ *
+ * All entry points are reentrant: each call uses its own CUDA stream.  On the
+ * GPU the library needs a CUDA device of compute capability 10.0 (B200); there
+ * is no CPU fallback.
+ */
+#ifndef CORRUSCANT_B200_KDTREE_H
+#define CORRUSCANT_B200_KDTREE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NDIM 3
+
+/* src/kdtree.h:13-17: a point; field and weight are 8-bit */
+typedef struct datum {
+    double value[NDIM];
+    unsigned int field:8;
+    unsigned int weight:8;
+} datum_t;
+
+/* src/kdtree.h:19-25: a heap node holding one point */
+typedef struct node {
+    datum_t data;
+    unsigned int has_lchild:1;
+    unsigned int has_rchild:1;
+    unsigned int dim:8;
+} node_t;
+
+/* src/kdtree.h:27-31 (kept for source compatibility; unused by the ABI) */
+typedef struct field_counter {
+    long long total;
+    long long *array;
+    int num_fields;
+} field_counter_t;
+
+/* src/kdtree.h:33-41.  size = unique points; data, fields and args are NULL
+ * (the reference frees them before returning, kdbuild.c:530-534). */
+typedef struct kdtree {
+    node_t *node_data;
+    int size;
+    int memsize;
+    int num_fields;
+    datum_t *data;
+    int *fields;
+    int *args[NDIM];
+} kdtree_t;
+
+/* ---------------------------------------------------------------- reference ABI */
+
+/* Replaces tree_construct (src/kdtree.h:43, src/kdbuild.c:451-537).
+ * xyz: n interleaved (x,y,z) doubles; fields: n ints or NULL; the tree stores
+ * the low 8 bits of a field, like the reference's field:8.  Duplicated points
+ * are merged into one node whose weight counts them and whose field is the
+ * field of the first occurrence.  The node array is bit-identical in its
+ * semantic fields to the reference build's.
+ * On error (NaN coordinate, a point repeated 256+ times, n < 1, no device)
+ * returns a tree with node_data == NULL and size == 0; kd_last_error() says
+ * why.  The reference prints and exits in these cases (kdbuild.c:73-79,
+ * :508-511). */
+kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields);
+
+/* Replaces pair_count (src/kdtree.h:45, src/kdquery.c:165-249).
+ * Counts, for the `length` query points (interleaved xyz, NaN rows count
+ * nothing), the tree points within distance r: fl(d2) < fl(r*r) with d2
+ * evaluated in the reference's operation order, weighted by node weight.
+ * Returns a malloc'd array of num_fields * tree.num_fields counts, indexed
+ * qfield * num_fields + tfield as in kdquery.c:34 (free with kd_free_counts
+ * or free()).  num_threads is accepted and ignored.  Returns NULL on error:
+ * negative r (the reference's prune is undefined there), negative query
+ * fields, field ids that would index outside the array, or a device error. */
+long long *pair_count(kdtree_t tree, double *data, int *fields, int length,
+                      int num_fields, double r, int num_threads);
+
+/* Replaces destroy (src/kdbuild.c:303-306): releases the host node array and
+ * the tree's device memory. */
+void destroy(kdtree_t tree);
+
+/* ---------------------------------------------------------------- additions */
+
+#define KD_MODE_MIXED 0 /* FP32 distances + FP64 recheck near edges (default) */
+#define KD_MODE_FP64 1  /* every distance in FP64 */
+
+typedef struct kd_count_stats {
+    long long pairs_tested;    /* distances evaluated in tiles */
+    long long pairs_rechecked; /* pairs recomputed in FP64 after an FP32 band hit */
+    long long pairs_accepted;  /* pairs binned by whole node pairs, no distance */
+    long long pairs_wide;      /* pairs of tiles spanning more than 4 edges */
+    long long edge_pairs;      /* sum over tested pairs of the edges each was binned against */
+    long long warp_tiles;      /* (32 queries, tree run) tiles computed */
+    long long entries;         /* (query block, tree run) tiles listed */
+    double ms_traverse;        /* device time: node-pair traversal */
+    double ms_tiles;           /* device time: tile kernels */
+    double ms_total;           /* device time: whole count */
+    int tile_launches;
+    int launches;              /* kernel launches of the count */
+} kd_count_stats;
+
+/* Last error of the calling thread: returns its code (0 = none) and copies
+ * the message into buf (may be NULL). */
+int kd_last_error(char *buf, int len);
+
+/* Frees an array returned by pair_count. */
+void kd_free_counts(long long *counts);
+
+/* Multi-radius count with another tree's points as the queries (its raw
+ * input points, duplicates included, each with its own field): for every
+ * radius k, out[k*Fq*Ft + qf*Fq + tf] is what pair_count(tree,
+ * query_points, query_fields, n, Fq, radii[k], .) returns, with
+ * Fq = query.num_fields and Ft = tree.num_fields.  All radii are counted in
+ * one pass over the node pairs.  Replaces the per-edge pair_count loop of
+ * clustering.py:218-230, :256-284.  mode: KD_MODE_MIXED or KD_MODE_FP64.
+ * stats may be NULL.  Returns 0 or a negative error code. */
+int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii,
+                   int nradii, int mode, long long *out, kd_count_stats *stats);
+
+/* Same, with arbitrary query points (interleaved xyz, fields may be NULL). */
+int kd_count_points(kdtree_t tree, const double *xyz, const int *fields,
+                    int length, int num_fields, const double *radii,
+                    int nradii, int mode, long long *out,
+                    kd_count_stats *stats);
+
+/* In-order permutation of the tree: perm[i] = index, in the input array
+ * given to tree_construct, of the (first occurrence of the) point stored at
+ * in-order position i.  perm holds tree.size ints. */
+int kd_tree_permutation(kdtree_t tree, int *perm);
+
+/* Raw (input) point count of a tree, duplicates included. */
+int kd_tree_input_size(kdtree_t tree);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
