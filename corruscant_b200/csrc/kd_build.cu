@@ -900,13 +900,14 @@ __global__ void k_block_fill(int nb_nodes, int span, const int *__restrict__ lea
     }
 }
 
-// one CTA of KD_BLOCK_MAX threads per query block
+// one CTA of KD_BLOCK_MAX threads per query block: box and single own field
 __global__ void __launch_bounds__(KD_BLOCK_MAX) k_block_boxes(int nblocks, const int *bstart,
                                                              const int *blen, RawOut o,
-                                                             double *bbox, double *wbox, int *bqf)
+                                                             double *bbox, int *bqf)
 {
-    __shared__ double sw[KD_WARPS][6];
-    __shared__ int sq[KD_WARPS];
+    constexpr int W = KD_BLOCK_MAX / 32;
+    __shared__ double sw[W][6];
+    __shared__ int sq[W];
     int b = blockIdx.x;
     if (b >= nblocks) return;
     int t = threadIdx.x, w = t >> 5, lane = t & 31;
@@ -931,8 +932,6 @@ __global__ void __launch_bounds__(KD_BLOCK_MAX) k_block_boxes(int nblocks, const
         for (int d = 0; d < 3; d++) {
             sw[w][d] = lo[d];
             sw[w][3 + d] = hi[d];
-            wbox[((size_t)b * KD_WARPS + w) * 6 + d] = lo[d];
-            wbox[((size_t)b * KD_WARPS + w) * 6 + 3 + d] = hi[d];
         }
         sq[w] = (32 * w >= len) ? -2 : (mixed ? -1 : q0);
     }
@@ -940,7 +939,7 @@ __global__ void __launch_bounds__(KD_BLOCK_MAX) k_block_boxes(int nblocks, const
     if (t == 0) {
         double L[3] = {INFINITY, INFINITY, INFINITY}, H[3] = {-INFINITY, -INFINITY, -INFINITY};
         int q = -2;
-        for (int k = 0; k < KD_WARPS; k++) {
+        for (int k = 0; k < W; k++) {
             for (int d = 0; d < 3; d++) {
                 L[d] = fmin(L[d], sw[k][d]);
                 H[d] = fmax(H[d], sw[k][3 + d]);
@@ -1308,8 +1307,8 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         memcpy(&leaf_hdiag, &hb, sizeof leaf_hdiag);
     }
 
-    // query blocks
-    int DB = std::max(0, D - 3);
+    // query blocks: each 16-leaf subtree cut into equal chunks of <= 128
+    int DB = std::max(0, D - 4);
     int nbn = 1 << DB, span = nleaves / nbn;
     int *nblk = pool.alloc<int>(nbn + 1), *boff = pool.alloc<int>(nbn + 1);
     k_block_count<<<blocks_for(nbn, TPB), TPB, 0, s>>>(nbn, span, leaf_r, nblk);
@@ -1318,10 +1317,9 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     int nblocks = read1(boff + nbn, s);
     int *bstart = keep.alloc<int>(nblocks), *blen = keep.alloc<int>(nblocks),
         *bqf = keep.alloc<int>(nblocks);
-    double *bbox = keep.alloc<double>(6 * (size_t)nblocks),
-           *wbox = keep.alloc<double>(6 * (size_t)KD_WARPS * nblocks);
+    double *bbox = keep.alloc<double>(6 * (size_t)nblocks);
     k_block_fill<<<blocks_for(nbn, TPB), TPB, 0, s>>>(nbn, span, leaf_r, nblk, boff, bstart, blen);
-    k_block_boxes<<<nblocks, KD_BLOCK_MAX, 0, s>>>(nblocks, bstart, blen, ro, bbox, wbox, bqf);
+    k_block_boxes<<<nblocks, KD_BLOCK_MAX, 0, s>>>(nblocks, bstart, blen, ro, bbox, bqf);
     KD_LAUNCH_CHECK("summary kernels");
     st.sync();
 
@@ -1364,7 +1362,6 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     cat->d_blk_len = keep.keep(blen);
     cat->d_blk_qf = keep.keep(bqf);
     cat->d_blk_box = keep.keep(bbox);
-    cat->d_blk_wbox = keep.keep(wbox);
     cat->device_bytes = keep.bytes;
 }
 
@@ -1425,8 +1422,7 @@ extern "C" void kdg_free(kd_catalog *cat)
                     cat->d_box,      cat->d_ncount,      cat->d_ntf,     cat->d_nqf,
                     cat->d_leaf_run, cat->d_run_start,   cat->d_run_len, cat->d_run_tf,
                     cat->d_run_leaf, cat->d_t4,          cat->d_leaf_c,
-                    cat->d_blk_start, cat->d_blk_len,    cat->d_blk_qf,  cat->d_blk_box,
-                    cat->d_blk_wbox};
+                    cat->d_blk_start, cat->d_blk_len,    cat->d_blk_qf,  cat->d_blk_box};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     memset(cat, 0, sizeof *cat);

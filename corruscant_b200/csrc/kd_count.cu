@@ -1,33 +1,34 @@
 // Pair counting for corruscant's pair_count (kdquery.c:62-113, :165-249),
 // batched over all bin edges at once.
 //
-// Semantics kept from the reference (proved equivalent in DESIGN.md): the
-// reference traversal counts, for every query point q and every tree node t,
-// weight(t) if fl(d2) < fl(r*r), where d2 is evaluated as
+// Semantics kept from the reference: the reference traversal counts, for
+// every query point q and every tree node t, weight(t) if fl(d2) < fl(r*r),
+// where d2 is evaluated as
 //     dx = t.x - q.x, ...;  d2 = dx*dx;  d2 = fma(dy,dy,d2);  d2 = fma(dz,dz,d2)
-// (kdquery.c:39-47 as the reference build compiles it) and its pruning
+// (kdquery.c:39-47 as the reference build compiles it), and its pruning
 // (kdquery.c:96-104) never drops such a pair.  Here a pair lands in bin e, the
 // first sorted squared edge with d2 < rsq[e]; cumulative sums over e give the
 // reference's per-radius counts.
 //
 // Work decomposition (B200-first, not the reference's per-query recursion):
-//   k_traverse : one warp per query block walks the tree-side counting tree
-//                with box-box distance bounds.  Node pairs beyond the last
-//                edge are pruned, node pairs entirely inside one bin are
-//                accepted as count(block) x count(node), and leaf pairs are
-//                emitted as tiles (block, run) with a per-warp active edge
-//                range.  Run twice: once to count tiles, once to write them.
-//   k_tiles    : one CTA (8 warps, one query point per thread) per query
-//                block streams its tree runs through shared memory (double
-//                buffered, one barrier per run).  Mixed mode: FP32 distances
-//                relative to the block centre, binned against the active edges
-//                with a saturating ramp that is exactly 0 or 1 outside a
-//                rigorous error band; a tile with any pair inside the band is
-//                recomputed for that thread in FP64 with the reference's
-//                operation order.  FP64 mode: every distance in FP64.
-//                Per-thread bin counters live in shared memory and are
-//                reduced per warp into the global (bin, qfield, tfield)
-//                histogram when the tree field changes.
+//   k_traverse : one warp per query block (<= 128 points) walks the tree-side
+//                counting tree with box-box distance bounds.  Node pairs
+//                beyond the last edge are pruned, node pairs inside one bin
+//                are accepted as count(block) x count(node), and leaf pairs
+//                become tile records (tree run, active edge range).  Run twice:
+//                once to count the tiles, once to write them.
+//   k_tiles    : one warp per query block, four query points per lane, walks
+//                its tile records.  Each tree run is staged into the warp's
+//                shared memory (the next run's loads already in flight) and
+//                every staged point is compared with the lane's four queries.
+//                Mixed mode: FP32 distances relative to the block centre,
+//                binned against the active edges with a saturating ramp that
+//                is exactly 0 or 1 outside a rigorous error band; a query
+//                with any pair of the run inside the band is recounted in
+//                FP64 with the reference's operation order.  FP64 mode: every
+//                distance in FP64.  Per-query bin counters live in shared
+//                memory and are reduced per (own field) into the global
+//                (bin, qfield, tfield) histogram when the tree field changes.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -40,7 +41,10 @@ namespace kd {
 
 constexpr int kTravWarps = 4;
 constexpr int kStack = 2048;
-constexpr int kTileThreads = KD_BLOCK_MAX;
+constexpr int kQ = KD_QPL;              // query points per lane
+constexpr int kTileWarpsPerCta = 4;
+constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
+constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
 
 struct TreeSide {
     const double *x, *y, *z;
@@ -54,7 +58,7 @@ struct QuerySide {
     const double *x, *y, *z;
     const int *qf;
     const int *blk_start, *blk_len, *blk_qf;
-    const double *blk_box, *blk_wbox;
+    const double *blk_box;
 };
 
 // Bins a pair of boxes can reach: pairs land in bins elo..ehi (ne = beyond
@@ -90,11 +94,12 @@ __device__ __forceinline__ void bin_range(const double *a, const double *b,
     ehi = l;
 }
 
+// A tile record: x = run start, y = leaf, z = run length | tree field << 8 |
+// first active edge << 16 | active edge count << 24.
 struct TravOut {
-    int *count;                 // COUNT pass: tiles per block
-    const long long *off;       // FILL pass: batch-relative tile offsets
-    unsigned *run;              // FILL: tree run of each tile
-    unsigned short *code;       // FILL: KD_WARPS codes per tile (k0 | K << 8)
+    int *count;              // COUNT pass: tiles per block
+    const long long *off;    // FILL pass: batch-relative tile offsets
+    uint4 *rec;              // FILL: tile records
     unsigned long long *H;
     int Fqe, Fte;
     unsigned long long *accepted;
@@ -108,43 +113,41 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
 {
     __shared__ int stack[kTravWarps][kStack];
     __shared__ double rsq[KD_MAX_EDGES];
-    __shared__ double wb[kTravWarps][KD_WARPS * 6 + 6];
+    __shared__ double wb[kTravWarps][6];
     for (int k = threadIdx.x; k < ne; k += blockDim.x) rsq[k] = g_rsq[k];
     __syncthreads();
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int b = b0 + blockIdx.x * kTravWarps + w;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int b = b0 + blockIdx.x * kTravWarps + w;
     if (b >= b1) return;
-    int alen = Q.blk_len[b], aqf = Q.blk_qf[b];
-    int nw = (alen + 31) >> 5;
+    const int alen = Q.blk_len[b], aqf = Q.blk_qf[b];
     double *bb = wb[w];
-    for (int k = lane; k < 6; k += 32) bb[k] = Q.blk_box[6 * (size_t)b + k];
-    for (int k = lane; k < KD_WARPS * 6; k += 32) bb[6 + k] = Q.blk_wbox[(size_t)b * KD_WARPS * 6 + k];
+    if (lane < 6) bb[lane] = Q.blk_box[6 * (size_t)b + lane];
     int *st = stack[w];
     if (lane == 0) st[0] = 1;
     __syncwarp();
     int sp = 1;
     long long emitted = 0;
-    long long base = FILL ? o.off[b - b0] : 0;
+    const long long base = FILL ? o.off[b - b0] : 0;
     unsigned long long acc_pairs = 0;
-    long long guard = 8LL * 2 * T.nleaves + 64;
+    long long guard = 4LL * T.nleaves + 64;
     while (sp > 0) {
         if (--guard < 0) {
             if (lane == 0) atomicCAS(o.err, 0, KD_EINTERNAL);
             break;
         }
-        int nb = min(sp, 32);
-        int h = lane < nb ? st[sp - nb + lane] : 0;
+        const int nb = min(sp, 32);
+        const int h = lane < nb ? st[sp - nb + lane] : 0;
         __syncwarp();
         sp -= nb;
-        int act = 0, nr = 0, leaf = 0;
+        int act = 0, nr = 0, leaf = 0, elo = 0, ehi = 0;
         if (h) {
-            int elo, ehi;
             bin_range(bb, T.box + 6 * (size_t)h, rsq, ne, elo, ehi);
             if (elo >= ne) {
                 act = 0;
             } else if (elo == ehi && aqf >= 0 && T.tf[h] >= 0) {
                 if (FILL) {
-                    unsigned long long c = (unsigned long long)alen * (unsigned long long)T.count[h];
+                    const unsigned long long c =
+                        (unsigned long long)alen * (unsigned long long)T.count[h];
                     atomicAdd(&o.H[((size_t)elo * o.Fqe + aqf) * o.Fte + T.tf[h]], c);
                     acc_pairs += c;
                 }
@@ -156,13 +159,12 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
                 act = 1;
             }
         }
-        int push = act == 1 ? 2 : 0;
-        int ps = push;
+        int ps = act == 1 ? 2 : 0;
         for (int off = 1; off < 32; off <<= 1) {
-            int v = __shfl_up_sync(0xffffffffu, ps, off);
+            const int v = __shfl_up_sync(0xffffffffu, ps, off);
             if (lane >= off) ps += v;
         }
-        int ptot = __shfl_sync(0xffffffffu, ps, 31);
+        const int ptot = __shfl_sync(0xffffffffu, ps, 31);
         if (sp + ptot > kStack) {
             if (lane == 0) atomicCAS(o.err, 0, KD_EINTERNAL);
             break;
@@ -174,33 +176,20 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
         sp += ptot;
         int es = act == 2 ? nr : 0;
         for (int off = 1; off < 32; off <<= 1) {
-            int v = __shfl_up_sync(0xffffffffu, es, off);
+            const int v = __shfl_up_sync(0xffffffffu, es, off);
             if (lane >= off) es += v;
         }
-        int etot = __shfl_sync(0xffffffffu, es, 31);
+        const int etot = __shfl_sync(0xffffffffu, es, 31);
         if (FILL && act == 2) {
-            unsigned short codes[KD_WARPS];
-            const double *tb = T.box + 6 * (size_t)h;
-            for (int ww = 0; ww < KD_WARPS; ww++) {
-                if (ww < nw) {
-                    int elo, ehi;
-                    bin_range(bb + 6 + 6 * ww, tb, rsq, ne, elo, ehi);
-                    codes[ww] = (unsigned short)(elo | ((ehi - elo) << 8));
-                } else {
-                    codes[ww] = (unsigned short)ne;
-                }
-            }
-            int r0 = T.leaf_run[leaf];
+            const unsigned code = (unsigned)elo | ((unsigned)(ehi - elo) << 8);
+            const int r0 = T.leaf_run[leaf];
             for (int k = 0; k < nr; k++) {
-                long long idx = base + emitted + es - nr + k;
-                o.run[idx] = (unsigned)(r0 + k);
-                uint4 *cp = (uint4 *)(o.code + idx * KD_WARPS);
-                uint4 v;
-                v.x = codes[0] | ((unsigned)codes[1] << 16);
-                v.y = codes[2] | ((unsigned)codes[3] << 16);
-                v.z = codes[4] | ((unsigned)codes[5] << 16);
-                v.w = codes[6] | ((unsigned)codes[7] << 16);
-                *cp = v;
+                const long long idx = base + emitted + es - nr + k;
+                const int r = r0 + k;
+                o.rec[idx] = make_uint4((unsigned)T.run_start[r], (unsigned)leaf,
+                                        (unsigned)T.run_len[r] | ((unsigned)T.run_tf[r] << 8) |
+                                            (code << 16),
+                                        0u);
             }
         }
         emitted += etot;
@@ -214,29 +203,29 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
 }
 
 // Rigorous half-width E of the uncertain band around edge R.
-// Geometry of a tile: query points within Rq of the warp centre o, tree points
-// within hT of their leaf centre c; both sides are re-centred on c in FP32:
-//   q' = fl(fl(q - o) - fl(c - o)),   t' = fl(t - c),   T = fl(|t'|^2),
-//   s  = fma(q'z, -2t'z, fma(q'y, -2t'y, fma(q'x, -2t'x, T)))   (= |t'-q'|^2 - |q'|^2)
-//   a  = fl(A - |q'|^2 / 4E),  A = fl(1/2 + R / 4E),   c = sat(a - s / 4E)
-// c is exactly 1 when s is more than 2E below R - |q'|^2, 0 when more than 2E
+// Geometry of a tile: query points within Rq of the block centre o; a tree
+// point t is stored as t_r = fl32(t - c) (c: its leaf's centre, |t - c| <= hT)
+// and staged as t' = fl32(t_r + fl32(c - o)); the query as q' = fl32(q - o);
+//   T = |t'|^2 (FP32 FMA chain),  s = T - 2 q'.t' (FP32 FMA chain),
+//   thr = R - |q'|^2,  c = sat(a - s/4E) with a = fl(A - |q'|^2/4E),
+//   A = fl(1/2 + R/4E).
+// c is exactly 1 when s is more than 2E below thr and 0 when more than 2E
 // above.  Every pair that is counted or lies within E of the edge has
-// d2 <= 2R, so |q - c| <= P = sqrt(2R) + hT, and for such pairs the FP32
-// quantity s - (R - |q'|^2) differs from d2 - R by at most
-//   u32 [ 2 sqrt(2R)(2P + 2Rq + hT) + 4 hT^2 + 6 P hT + 5 P^2 + 3 R ]
-// (coordinate rounding 2 sqrt(d2) eta with eta <= u32 (2P + 2Rq + hT), the
-// roundings of T, of the FMA chain for s and for |q'|^2, and of the threshold
-// a).  E adds 25%, a term for the FP64 reference's own rounding, and is rounded
+// d2 <= 2R, so |t - o| <= P = sqrt(2R) + Rq, and for such pairs
+//   |(s - thr) - (d2 - R)| <= u32 [2 (P + Rq)(2P + 2hT + Rq) + 6 P (P + Rq)
+//                                  + 3 (R + Rq^2)]
+// (coordinate rounding 2 sqrt(d2) eta with eta <= u32 (2P + 2hT + Rq), the
+// roundings of T and of the FMA chain for s, and those of the threshold).
+// E adds 25% and a term for the FP64 reference's own rounding, and is rounded
 // up to a power of two so that 1/(4E) is exact in FP32.  Pairs with d2 > 2R
-// have an FP32 value far above the band (its error grows like u32 d2).
+// sit far above the band: their FP32 error grows only like 10 u32 d2.
 __device__ __forceinline__ double band_halfwidth(double R, double Rq, double hT)
 {
     const double u32 = 5.9604644775390625e-08;  // 2^-24
-    const double sr = sqrt(2.0 * R);
-    const double P = sr + hT;
-    double e = 2.0 * sr * (2.0 * P + 2.0 * Rq + hT) + 4.0 * hT * hT + 6.0 * P * hT +
-               5.0 * P * P + 3.0 * R;
-    double E = 1.25 * u32 * e + 1e-15 * R + 1e-30;
+    const double P = sqrt(2.0 * R) + Rq;
+    const double e = 2.0 * (P + Rq) * (2.0 * P + 2.0 * hT + Rq) + 6.0 * P * (P + Rq) +
+                     3.0 * (R + Rq * Rq);
+    const double E = 1.25 * u32 * e + 1e-15 * R + 1e-30;
     int ex;
     frexp(E, &ex);
     return ldexp(1.0, ex);
@@ -250,66 +239,109 @@ __device__ __forceinline__ float fma_sat(float a, float b, float c)
     return d;
 }
 
-// FP32 pass of one lane's query over a run and K (<= 4) edges.  Each pair
-// gives c_k = sat(a_k + s * nsl_k), exactly 0 or 1 outside the band and in
-// [1/4, 3/4] inside it.  sum_k acc_k equals acc2 = sum c^2 bit for bit when
-// every c is 0 or 1; a band pair makes them differ by at least 3/16, far
-// above the FP32 rounding of these short sums (<= 256 terms of at most 1).
+// FP32 pass of a lane's four queries over a staged run and K (<= 4) edges.
+// Each pair gives c = sat(a_k + s * nsl_k): exactly 0 or 1 outside the band,
+// in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals acc2 = sum c^2 bit
+// for bit when every c is 0 or 1; a band pair makes them differ by at least
+// 3/16, far above the FP32 rounding of these short sums (<= 256 terms <= 1).
+// Returns a bit mask of the queries with a band pair.
 template <int K>
-__device__ __forceinline__ bool fp32_run(const float4 *__restrict__ t, int rl, float qx, float qy,
-                                         float qz, const float *a, const float *nsl, int *cnt)
+__device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int rl,
+                                             const float (&qx)[kQ], const float (&qy)[kQ],
+                                             const float (&qz)[kQ], const float (&a)[kQ][kPass32],
+                                             const float (&nsl)[kPass32], int (&cnt)[kQ][4])
 {
-    float acc[K], acc2 = 0.0f;
+    float acc[kQ][K], acc2[kQ];
 #pragma unroll
-    for (int k = 0; k < K; k++) acc[k] = 0.0f;
+    for (int p = 0; p < kQ; p++) {
+        acc2[p] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; k++) acc[p][k] = 0.0f;
+    }
     int j = 0;
     for (; j + 2 <= rl; j += 2) {
-        const float4 t0 = __ldg(t + j), t1 = __ldg(t + j + 1);
-        const float s0 = fmaf(qz, t0.z, fmaf(qy, t0.y, fmaf(qx, t0.x, t0.w)));
-        const float s1 = fmaf(qz, t1.z, fmaf(qy, t1.y, fmaf(qx, t1.x, t1.w)));
+        const float4 t[2] = {ts[j], ts[j + 1]};
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            const float c0 = fma_sat(s0, nsl[k], a[k]);
-            const float c1 = fma_sat(s1, nsl[k], a[k]);
-            acc[k] += c0;
-            acc2 = fmaf(c0, c0, acc2);
-            acc[k] += c1;
-            acc2 = fmaf(c1, c1, acc2);
-        }
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+            for (int p = 0; p < kQ; p++) {
+                const float s = fmaf(qz[p], t[u].z, fmaf(qy[p], t[u].y, fmaf(qx[p], t[u].x, t[u].w)));
+#pragma unroll
+                for (int k = 0; k < K; k++) {
+                    const float c = fma_sat(s, nsl[k], a[p][k]);
+                    acc[p][k] += c;
+                    acc2[p] = fmaf(c, c, acc2[p]);
+                }
+            }
     }
     if (j < rl) {
-        const float4 t0 = __ldg(t + j);
-        const float s0 = fmaf(qz, t0.z, fmaf(qy, t0.y, fmaf(qx, t0.x, t0.w)));
+        const float4 t = ts[j];
 #pragma unroll
-        for (int k = 0; k < K; k++) {
-            const float c0 = fma_sat(s0, nsl[k], a[k]);
-            acc[k] += c0;
-            acc2 = fmaf(c0, c0, acc2);
+        for (int p = 0; p < kQ; p++) {
+            const float s = fmaf(qz[p], t.z, fmaf(qy[p], t.y, fmaf(qx[p], t.x, t.w)));
+#pragma unroll
+            for (int k = 0; k < K; k++) {
+                const float c = fma_sat(s, nsl[k], a[p][k]);
+                acc[p][k] += c;
+                acc2[p] = fmaf(c, c, acc2[p]);
+            }
         }
     }
-    float tot = 0.0f;
+    unsigned band = 0;
 #pragma unroll
-    for (int k = 0; k < K; k++) {
-        tot += acc[k];
-        cnt[k] = __float2int_rn(acc[k]);
+    for (int p = 0; p < kQ; p++) {
+        float tot = 0.0f;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            tot += acc[p][k];
+            cnt[p][k] = __float2int_rn(acc[p][k]);
+        }
+        if (tot != acc2[p]) band |= 1u << p;
     }
-    return tot == acc2;
+    return band;
 }
 
 // reference-order FP64 distance (kdquery.c:39-47 as compiled)
 __device__ __forceinline__ double d2_ref(double tx, double ty, double tz, double qx, double qy,
                                          double qz)
 {
-    double dx = __dsub_rn(tx, qx), dy = __dsub_rn(ty, qy), dz = __dsub_rn(tz, qz);
+    const double dx = __dsub_rn(tx, qx), dy = __dsub_rn(ty, qy), dz = __dsub_rn(tz, qz);
     double s = __dmul_rn(dx, dx);
     s = __fma_rn(dy, dy, s);
     return __fma_rn(dz, dz, s);
 }
 
-// Exact pass in FP64 with the reference's operation order: cumulative counts
-// of pairs with d2 < R[k] for the kn (<= 4) edges, packed one per byte (a run
-// has at most KD_RUN_MAX = 64 points).  Used for FP64 mode, band rechecks and
-// infinite radii; kept out of line so the FP32 loop stays small.
+// FP64 pass of the four queries over a staged run (FP64 mode): cumulative
+// counts for K (<= 4) edges.
+template <int K>
+__device__ __forceinline__ void fp64_run(const double *__restrict__ tx,
+                                         const double *__restrict__ ty,
+                                         const double *__restrict__ tz, int rl,
+                                         const double (&qx)[kQ], const double (&qy)[kQ],
+                                         const double (&qz)[kQ], const double *R,
+                                         int (&cnt)[kQ][4])
+{
+    double r[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) r[k] = R[k];
+#pragma unroll
+    for (int p = 0; p < kQ; p++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) cnt[p][k] = 0;
+    for (int j = 0; j < rl; j++) {
+        const double x = tx[j], y = ty[j], z = tz[j];
+#pragma unroll
+        for (int p = 0; p < kQ; p++) {
+            const double d2 = d2_ref(x, y, z, qx[p], qy[p], qz[p]);
+#pragma unroll
+            for (int k = 0; k < K; k++) cnt[p][k] += d2 < r[k];
+        }
+    }
+}
+
+// Exact recount of one query over a run (global FP64 coordinates), for band
+// rechecks and edges FP32 cannot represent; counts packed one per byte.  Out
+// of line so the FP32 loop stays small.
 __device__ __noinline__ unsigned exact_pass(const double *__restrict__ tx,
                                             const double *__restrict__ ty,
                                             const double *__restrict__ tz, int rl, double qx,
@@ -327,72 +359,98 @@ __device__ __noinline__ unsigned exact_pass(const double *__restrict__ tx,
 }
 
 struct TileArgs {
-    TreeSide T;
-    const float4 *t4;     // tree points: (-2t, |t|^2), t relative to the leaf centre
-    const int *run_leaf;
-    const double *leaf_c; // 3 per leaf
-    double hT;            // largest leaf half-diagonal
+    const double *tx, *ty, *tz;  // tree points, FP64, counting order
+    const float4 *t4;            // tree points: (-2 t_r, |t_r|^2), t_r relative to leaf centre
+    const double *leaf_c;        // 3 per leaf
+    double hT;                   // largest leaf half-diagonal
     QuerySide Q;
     const double *rsq;
     int ne;
     int b0, b1;
     const long long *off;
-    const unsigned *run;
-    const unsigned short *code;
+    const uint4 *rec;
     unsigned long long *H;
     int Fqe, Fte;
     int *work;
     unsigned long long *stats;  // tested, rechecked, accepted, wide, edge-pairs, warp tiles
 };
 
-constexpr int kTileWarps = KD_BLOCK_MAX / 32;
+// shared memory of one warp
+template <int MODE> struct WarpSmem {
+    float Aw[KD_MAX_EDGES];
+    float nsl[KD_MAX_EDGES];
+    int uq[kMaxDistinctQf];
+    float4 stage[MODE == KD_MODE_MIXED ? KD_RUN_MAX : 1];
+    double stage64[MODE == KD_MODE_FP64 ? 3 * KD_RUN_MAX : 1];
+};
 
-// One warp = one work item: 32 query points (a warp's slice of a query block)
-// against that block's list of tree runs.  Warps never wait for each other;
-// tree points are read with broadcast loads (the block's 8 warps walk the
-// same runs, so they hit in L1).
 template <int MODE>
-__global__ void __launch_bounds__(32 * kTileWarps, 3) k_tiles(TileArgs A)
+__global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     const int ne = A.ne;
-    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
-    int *P = (int *)smem;                                           // (ne+1) x 256
-    double *R = (double *)(P + (size_t)(ne + 1) * kTileThreads);    // ne
-    float *Aw = (float *)(R + KD_MAX_EDGES) + w * 2 * KD_MAX_EDGES; // per warp: A_k
-    float *nsl = Aw + KD_MAX_EDGES;                                 //           -1/(4E_k)
-
-    for (int k = tid; k < ne; k += blockDim.x) R[k] = A.rsq[k];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *R = (double *)smem;  // ne
+    WarpSmem<MODE> *ws = (WarpSmem<MODE> *)(R + KD_MAX_EDGES) + w;
+    // per-query bin counters: P[(e * kQ + p) * 32 + lane]
+    int *P = (int *)((WarpSmem<MODE> *)(R + KD_MAX_EDGES) + kTileWarpsPerCta) +
+             (size_t)w * (ne + 1) * kQ * 32;
+    for (int k = threadIdx.x; k < ne; k += blockDim.x) R[k] = A.rsq[k];
     __syncthreads();
     unsigned long long pairs = 0, rechecked = 0, wide = 0, kpairs = 0, wtiles = 0;
-    int *Pt = P + tid;
 
     while (true) {
         int item = 0;
         if (lane == 0) item = atomicAdd(A.work, 1);
         item = __shfl_sync(0xffffffffu, item, 0);
-        const int b = A.b0 + item / kTileWarps, wi = item % kTileWarps;
+        const int b = A.b0 + item;
         if (b >= A.b1) break;
-        const int qlen = A.Q.blk_len[b] - 32 * wi;
-        if (qlen <= 0) continue;
-        const int qs = A.Q.blk_start[b] + 32 * wi;
+        const int qlen = A.Q.blk_len[b], qs = A.Q.blk_start[b];
         const long long eoff = A.off[b - A.b0];
         const int ecnt = (int)(A.off[b - A.b0 + 1] - eoff);
-        const double *bx = A.Q.blk_wbox + ((size_t)b * KD_WARPS + wi) * 6;
+        const double *bx = A.Q.blk_box + 6 * (size_t)b;
         const double ox = 0.5 * (bx[0] + bx[3]), oy = 0.5 * (bx[1] + bx[4]),
                      oz = 0.5 * (bx[2] + bx[5]);
-        const bool valid = lane < qlen;
-        double qxd = ox, qyd = oy, qzd = oz;
-        int qf = 0;
-        if (valid) {
-            qxd = A.Q.x[qs + lane];
-            qyd = A.Q.y[qs + lane];
-            qzd = A.Q.z[qs + lane];
-            qf = A.Q.qf[qs + lane];
+        // queries 4*lane .. 4*lane+3 of the block; their FP64 coordinates and
+        // own fields are re-read from global memory when needed (exact
+        // recounts, flushes) instead of being held in registers
+        const int qbase = qs + kQ * lane;
+        float qx[kQ], qy[kQ], qz[kQ], qn[kQ];
+        unsigned vmask = 0;
+#pragma unroll
+        for (int p = 0; p < kQ; p++) {
+            const int j = kQ * lane + p;
+            const bool v = j < qlen;
+            vmask |= (unsigned)v << p;
+            const double xd = v ? A.Q.x[qs + j] : ox, yd = v ? A.Q.y[qs + j] : oy,
+                         zd = v ? A.Q.z[qs + j] : oz;
+            qx[p] = (float)(xd - ox);
+            qy[p] = (float)(yd - oy);
+            qz[p] = (float)(zd - oz);
+            qn[p] = (float)((double)qx[p] * qx[p] + (double)qy[p] * qy[p] + (double)qz[p] * qz[p]);
         }
-        const int q0 = __shfl_sync(0xffffffffu, qf, 0);
-        const int wq = __all_sync(0xffffffffu, !valid || qf == q0) ? q0 : -1;
-        const float qwx = (float)(qxd - ox), qwy = (float)(qyd - oy), qwz = (float)(qzd - oz);
+        const int nvalid = __popc(vmask);
+        auto qfield = [&](int p) { return ((vmask >> p) & 1) ? A.Q.qf[qbase + p] : -1; };
+        // the distinct own fields of the block (up to kMaxDistinctQf are
+        // reduced per warp at a flush; beyond that, per-query atomics)
+        int nuq = 0;
+        {
+            unsigned todo = vmask;
+            for (int round = 0; round <= kQ * 32; round++) {
+                int cand = -1;
+#pragma unroll
+                for (int p = 0; p < kQ; p++)
+                    if (cand < 0 && ((todo >> p) & 1)) cand = qfield(p);
+                const unsigned any = __ballot_sync(0xffffffffu, cand >= 0);
+                if (!any) break;
+                const int pick = __shfl_sync(0xffffffffu, cand, __ffs(any) - 1);
+                if (nuq < kMaxDistinctQf && lane == 0) ws->uq[nuq] = pick;
+                nuq++;
+#pragma unroll
+                for (int p = 0; p < kQ; p++)
+                    if (((todo >> p) & 1) && qfield(p) == pick) todo &= ~(1u << p);
+            }
+        }
         if (MODE == KD_MODE_MIXED) {
             const double hx = 0.5 * (bx[3] - bx[0]), hy = 0.5 * (bx[4] - bx[1]),
                          hz = 0.5 * (bx[5] - bx[2]);
@@ -400,40 +458,119 @@ __global__ void __launch_bounds__(32 * kTileWarps, 3) k_tiles(TileArgs A)
             for (int k = lane; k < ne; k += 32) {
                 if (isfinite(R[k])) {
                     const double inv4e = 0.25 / band_halfwidth(R[k], Rq, A.hT);
-                    nsl[k] = (float)(-inv4e);
-                    Aw[k] = (float)(0.5 + R[k] * inv4e);
+                    ws->nsl[k] = (float)(-inv4e);
+                    ws->Aw[k] = (float)(0.5 + R[k] * inv4e);
                 } else {
-                    nsl[k] = 0.0f;
-                    Aw[k] = 0.0f;
+                    ws->nsl[k] = 0.0f;
+                    ws->Aw[k] = 0.0f;
                 }
             }
         }
-        for (int e = 0; e <= ne; e++) Pt[(size_t)e * kTileThreads] = 0;
+        for (int e = 0; e <= ne; e++)
+#pragma unroll
+            for (int p = 0; p < kQ; p++) P[(e * kQ + p) * 32 + lane] = 0;
         __syncwarp();
         int cur_tf = -1;
         long long since = 0;
 
         auto flush = [&](int tf) {
+            int qf[kQ];
+#pragma unroll
+            for (int p = 0; p < kQ; p++) qf[p] = qfield(p);
             for (int e = 0; e < ne; e++) {
-                int v = Pt[(size_t)e * kTileThreads];
-                Pt[(size_t)e * kTileThreads] = 0;
-                if (wq >= 0) {
-                    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-                    if (lane == 0 && v)
-                        atomicAdd(&A.H[((size_t)e * A.Fqe + wq) * A.Fte + tf], (unsigned long long)v);
-                } else if (valid && v) {
-                    atomicAdd(&A.H[((size_t)e * A.Fqe + qf) * A.Fte + tf], (unsigned long long)v);
+                int v[kQ];
+#pragma unroll
+                for (int p = 0; p < kQ; p++) {
+                    v[p] = P[(e * kQ + p) * 32 + lane];
+                    P[(e * kQ + p) * 32 + lane] = 0;
+                }
+                if (nuq <= kMaxDistinctQf) {
+                    for (int u = 0; u < nuq; u++) {
+                        const int uf = ws->uq[u];
+                        int sum = 0;
+#pragma unroll
+                        for (int p = 0; p < kQ; p++) sum += qf[p] == uf ? v[p] : 0;
+                        for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                        if (lane == 0 && sum)
+                            atomicAdd(&A.H[((size_t)e * A.Fqe + uf) * A.Fte + tf],
+                                      (unsigned long long)sum);
+                    }
+                } else {
+#pragma unroll
+                    for (int p = 0; p < kQ; p++)
+                        if (((vmask >> p) & 1) && v[p])
+                            atomicAdd(&A.H[((size_t)e * A.Fqe + qf[p]) * A.Fte + tf],
+                                      (unsigned long long)v[p]);
                 }
             }
-            Pt[(size_t)ne * kTileThreads] = 0;
+#pragma unroll
+            for (int p = 0; p < kQ; p++) P[(ne * kQ + p) * 32 + lane] = 0;
         };
 
+        // the next record's loads, held in registers while the current run
+        // is counted
+        uint4 nrec = make_uint4(0, 0, 0, 0);
+        float4 na = make_float4(0, 0, 0, 0), nb = na;
+        double ncx = 0, ncy = 0, ncz = 0;
+        auto issue = [&](int i) {
+            nrec = A.rec[eoff + i];
+            const int rl = nrec.z & 0xFF, K = nrec.z >> 24;
+            if (K == 0) return;
+            if (MODE == KD_MODE_MIXED) {
+                const unsigned rs = nrec.x, leaf = nrec.y;
+                ncx = A.leaf_c[3 * (size_t)leaf];
+                ncy = A.leaf_c[3 * (size_t)leaf + 1];
+                ncz = A.leaf_c[3 * (size_t)leaf + 2];
+                if (lane < rl) na = A.t4[rs + lane];
+                if (lane + 32 < rl) nb = A.t4[rs + lane + 32];
+            } else {
+                const unsigned rs = nrec.x;
+                if (lane < rl) {
+                    ncx = A.tx[rs + lane];
+                    ncy = A.ty[rs + lane];
+                    ncz = A.tz[rs + lane];
+                }
+            }
+        };
+
+        if (ecnt > 0) issue(0);
         for (int i = 0; i < ecnt; i++) {
-            const unsigned code = A.code[(eoff + i) * KD_WARPS + wi];
-            const int k0 = code & 0xFF, K = code >> 8;
-            if (k0 >= ne) continue;  // beyond every edge for this warp
-            const unsigned run = A.run[eoff + i];
-            const int rs = A.T.run_start[run], rl = A.T.run_len[run], tf = A.T.run_tf[run];
+            const uint4 rec = nrec;
+            const int rs = (int)rec.x, rl = rec.z & 0xFF, tf = (rec.z >> 8) & 0xFF;
+            const int k0 = (rec.z >> 16) & 0xFF, K = rec.z >> 24;
+            // commit the staged run
+            if (K != 0) {
+                if (MODE == KD_MODE_MIXED) {
+                    const float dx = (float)(ncx - ox), dy = (float)(ncy - oy), dz = (float)(ncz - oz);
+                    const float4 v2[2] = {na, nb};
+#pragma unroll
+                    for (int h = 0; h < 2; h++) {
+                        const int j = lane + 32 * h;
+                        if (j < rl) {
+                            // t' = t_r + (c - o); -0.5 * (-2 t_r) is exact
+                            const float lx = fmaf(-0.5f, v2[h].x, dx);
+                            const float ly = fmaf(-0.5f, v2[h].y, dy);
+                            const float lz = fmaf(-0.5f, v2[h].z, dz);
+                            ws->stage[j] = make_float4(-2.0f * lx, -2.0f * ly, -2.0f * lz,
+                                                       fmaf(lz, lz, fmaf(ly, ly, lx * lx)));
+                        }
+                    }
+                } else {
+                    if (lane < rl) {
+                        ws->stage64[lane] = ncx;
+                        ws->stage64[KD_RUN_MAX + lane] = ncy;
+                        ws->stage64[2 * KD_RUN_MAX + lane] = ncz;
+                    }
+                    for (int j = lane + 32; j < rl; j += 32) {
+                        ws->stage64[j] = A.tx[rs + j];
+                        ws->stage64[KD_RUN_MAX + j] = A.ty[rs + j];
+                        ws->stage64[2 * KD_RUN_MAX + j] = A.tz[rs + j];
+                    }
+                }
+            }
+            __syncwarp();
+            if (i + 1 < ecnt) issue(i + 1);
+
             if (tf != cur_tf || since > (1LL << 30)) {
                 if (cur_tf >= 0) flush(cur_tf);
                 cur_tf = tf;
@@ -441,63 +578,87 @@ __global__ void __launch_bounds__(32 * kTileWarps, 3) k_tiles(TileArgs A)
             }
             since += rl;
             if (K == 0) {
-                if (valid) Pt[(size_t)k0 * kTileThreads] += rl;
+#pragma unroll
+                for (int p = 0; p < kQ; p++)
+                    if ((vmask >> p) & 1) P[(k0 * kQ + p) * 32 + lane] += rl;
+                __syncwarp();
                 continue;
             }
             wtiles++;
-            // edges k0 .. k0+K-1 in passes of at most four; pairs land in
-            // bins k0 .. k0+K (the last: beyond the active edges)
             const bool fp32 = MODE == KD_MODE_MIXED && isfinite(R[k0 + K - 1]);
-            float qx = 0.0f, qy = 0.0f, qz = 0.0f, qn = 0.0f;
-            if (fp32) {
-                const int leaf = A.run_leaf[run];
-                const float dx = (float)(A.leaf_c[3 * (size_t)leaf] - ox);
-                const float dy = (float)(A.leaf_c[3 * (size_t)leaf + 1] - oy);
-                const float dz = (float)(A.leaf_c[3 * (size_t)leaf + 2] - oz);
-                qx = qwx - dx;
-                qy = qwy - dy;
-                qz = qwz - dz;
-                qn = fmaf(qz, qz, fmaf(qy, qy, qx * qx));
-            }
-            if (!valid) continue;
-            int prev = 0;
-            for (int kb = 0; kb < K; kb += 4) {
-                const int kn = min(4, K - kb);
-                int cnt[4] = {0, 0, 0, 0};
-                bool ok = false;
+            int prev[kQ];
+#pragma unroll
+            for (int p = 0; p < kQ; p++) prev[p] = 0;
+            const int pw = MODE == KD_MODE_MIXED && fp32 ? kPass32 : 4;
+            for (int kb = 0; kb < K; kb += pw) {
+                const int kn = min(pw, K - kb);
+                int cnt[kQ][4];
+                unsigned redo = vmask;
                 if (fp32) {
-                    float a[4], sl[4];
+                    float a[kQ][kPass32], sl[kPass32];
 #pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        sl[k] = k < kn ? nsl[k0 + kb + k] : 0.0f;
-                        a[k] = k < kn ? fmaf(qn, sl[k], Aw[k0 + kb + k]) : 0.0f;
+                    for (int k = 0; k < kPass32; k++) {
+                        sl[k] = k < kn ? ws->nsl[k0 + kb + k] : 0.0f;
+                        const float Ak = k < kn ? ws->Aw[k0 + kb + k] : 0.0f;
+#pragma unroll
+                        for (int p = 0; p < kQ; p++) a[p][k] = fmaf(qn[p], sl[k], Ak);
                     }
-                    const float4 *t = A.t4 + rs;
+                    unsigned band;
                     switch (kn) {
-                    case 1: ok = fp32_run<1>(t, rl, qx, qy, qz, a, sl, cnt); break;
-                    case 2: ok = fp32_run<2>(t, rl, qx, qy, qz, a, sl, cnt); break;
-                    case 3: ok = fp32_run<3>(t, rl, qx, qy, qz, a, sl, cnt); break;
-                    default: ok = fp32_run<4>(t, rl, qx, qy, qz, a, sl, cnt); break;
+                    case 1: band = fp32_run<1>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
+                    case 2: band = fp32_run<2>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
+                    case 3: band = fp32_run<3>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
+                    default: band = fp32_run<4>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
                     }
-                    if (!ok) rechecked += rl;
-                }
-                if (!ok) {
-                    const unsigned pk = exact_pass(A.T.x + rs, A.T.y + rs, A.T.z + rs, rl, qxd, qyd,
-                                                   qzd, R + k0 + kb, kn);
+                    redo = band & vmask;
+                    rechecked += (unsigned long long)__popc(redo) * rl;
+                } else if (MODE == KD_MODE_FP64) {
+                    double qxd[kQ], qyd[kQ], qzd[kQ];
 #pragma unroll
-                    for (int k = 0; k < 4; k++) cnt[k] = (pk >> (8 * k)) & 0xFF;
+                    for (int p = 0; p < kQ; p++) {
+                        const bool v = (vmask >> p) & 1;
+                        qxd[p] = v ? A.Q.x[qbase + p] : ox;
+                        qyd[p] = v ? A.Q.y[qbase + p] : oy;
+                        qzd[p] = v ? A.Q.z[qbase + p] : oz;
+                    }
+                    const double *s64 = ws->stage64;
+                    switch (kn) {
+                    case 1: fp64_run<1>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
+                    case 2: fp64_run<2>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
+                    case 3: fp64_run<3>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
+                    default: fp64_run<4>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
+                    }
+                    redo = 0;
                 }
+                // exact FP64 recount of the queries FP32 could not decide
 #pragma unroll
-                for (int k = 0; k < 4; k++)
-                    if (k < kn) {
-                        Pt[(size_t)(k0 + kb + k) * kTileThreads] += cnt[k] - prev;
-                        prev = cnt[k];
+                for (int p = 0; p < kQ; p++)
+                    if ((redo >> p) & 1) {
+                        const unsigned pk =
+                            exact_pass(A.tx + rs, A.ty + rs, A.tz + rs, rl, A.Q.x[qbase + p],
+                                       A.Q.y[qbase + p], A.Q.z[qbase + p], R + k0 + kb, kn);
+#pragma unroll
+                        for (int k = 0; k < 4; k++) cnt[p][k] = (pk >> (8 * k)) & 0xFF;
+                    }
+#pragma unroll
+                for (int p = 0; p < kQ; p++)
+                    if ((vmask >> p) & 1) {
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            if (k < kn) {
+                                P[((k0 + kb + k) * kQ + p) * 32 + lane] += cnt[p][k] - prev[p];
+                                prev[p] = cnt[p][k];
+                            }
                     }
             }
-            Pt[(size_t)(k0 + K) * kTileThreads] += rl - prev;
-            if (K > 4) wide += rl;
-            kpairs += (unsigned long long)rl * K;
-            pairs += rl;
+#pragma unroll
+            for (int p = 0; p < kQ; p++)
+                if ((vmask >> p) & 1) P[((k0 + K) * kQ + p) * 32 + lane] += rl - prev[p];
+            const unsigned long long tp = (unsigned long long)nvalid * rl;
+            pairs += tp;
+            kpairs += tp * K;
+            if (K > 4) wide += tp;
+            __syncwarp();
         }
         if (cur_tf >= 0) flush(cur_tf);
         __syncwarp();
@@ -519,9 +680,10 @@ __global__ void __launch_bounds__(32 * kTileWarps, 3) k_tiles(TileArgs A)
 
 static size_t tile_smem(int ne, int mode)
 {
-    (void)mode;
-    return sizeof(int) * (size_t)(ne + 1) * kTileThreads + sizeof(double) * KD_MAX_EDGES +
-           sizeof(float) * 2 * KD_MAX_EDGES * kTileWarps;
+    const size_t ws = mode == KD_MODE_MIXED ? sizeof(WarpSmem<KD_MODE_MIXED>)
+                                            : sizeof(WarpSmem<KD_MODE_FP64>);
+    return sizeof(double) * KD_MAX_EDGES + ws * kTileWarpsPerCta +
+           sizeof(int) * (size_t)(ne + 1) * kQ * 32 * kTileWarpsPerCta;
 }
 
 struct Events {
@@ -575,7 +737,6 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     Q.blk_len = qc->d_blk_len;
     Q.blk_qf = qc->d_blk_qf;
     Q.blk_box = qc->d_blk_box;
-    Q.blk_wbox = qc->d_blk_wbox;
 
     const int Fqe = qc->max_qf + 1, Fte = tc->max_tf + 1;
     const size_t hsz = (size_t)(ne + 1) * Fqe * Fte;
@@ -600,38 +761,38 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     to.Fte = Fte;
     to.accepted = dstats + 2;
     to.err = err;
-    unsigned tgrid = blocks_for(nb, kTravWarps);
-    k_traverse<false><<<tgrid, 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0, nb, to);
+    k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0, nb, to);
     launches++;
     KD_LAUNCH_CHECK("k_traverse(count)");
     std::vector<int> hcnt(nb);
     check(cudaMemcpyAsync(hcnt.data(), cnt, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToHost, s),
           "D2H");
-    st.sync();
     int herr = 0;
-    check(cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+    check(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+    st.sync();
     if (herr) raise(herr, "node-pair traversal exceeded its stack");
 
-    // batches of query blocks whose tiles fit the tile buffer
+    // batches of query blocks whose tile records fit the buffer
     long long total = 0;
     for (int v : hcnt) total += v;
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
-    long long cap = std::max<long long>(1 << 20, std::min<long long>(256LL << 20, (long long)(freeb / 4 / 20)));
+    long long cap = std::max<long long>(
+        1 << 20, std::min<long long>(256LL << 20, (long long)(freeb / 4 / sizeof(uint4))));
     cap = std::min<long long>(cap, std::max<long long>(total, 1));
-    unsigned *run = pool.alloc<unsigned>(cap);
-    unsigned short *code = pool.alloc<unsigned short>(cap * KD_WARPS);
+    uint4 *rec = pool.alloc<uint4>(cap);
     long long *off = pool.alloc<long long>(nb + 1);
     std::vector<long long> hoff(nb + 1);
 
-    size_t smem = tile_smem(ne, mode);
+    const size_t smem = tile_smem(ne, mode);
     auto kern = mode == KD_MODE_MIXED ? k_tiles<KD_MODE_MIXED> : k_tiles<KD_MODE_FP64>;
     check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
           "smem attribute");
     int dev = 0, nsm = 148, occ = 1;
     check(cudaGetDevice(&dev), "cudaGetDevice");
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kTileThreads, smem), "occupancy");
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * kTileWarpsPerCta, smem),
+          "occupancy");
     occ = std::max(occ, 1);
 
     float ms_trav = 0, ms_tiles = 0;
@@ -649,8 +810,7 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
                               cudaMemcpyHostToDevice, s), "H2D");
         TravOut tf = to;
         tf.off = off;
-        tf.run = run;
-        tf.code = code;
+        tf.rec = rec;
         check(cudaEventRecord(ev.e[1], s), "event");
         k_traverse<true><<<blocks_for(b1 - b0, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne,
                                                                                       b0, b1, tf);
@@ -658,9 +818,10 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
         KD_LAUNCH_CHECK("k_traverse(fill)");
         check(cudaEventRecord(ev.e[2], s), "event");
         TileArgs ta;
-        ta.T = T;
+        ta.tx = tc->d_x;
+        ta.ty = tc->d_y;
+        ta.tz = tc->d_z;
         ta.t4 = (const float4 *)tc->d_t4;
-        ta.run_leaf = tc->d_run_leaf;
         ta.leaf_c = tc->d_leaf_c;
         ta.hT = tc->leaf_hdiag * (1.0 + 1e-12);
         ta.Q = Q;
@@ -669,16 +830,16 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
         ta.b0 = b0;
         ta.b1 = b1;
         ta.off = off;
-        ta.run = run;
-        ta.code = code;
+        ta.rec = rec;
         ta.H = H;
         ta.Fqe = Fqe;
         ta.Fte = Fte;
         ta.work = work;
         ta.stats = dstats;
         check(cudaMemsetAsync(work, 0, sizeof(int), s), "memset");
-        int grid = (int)std::min<long long>((long long)(b1 - b0), (long long)nsm * occ);
-        kern<<<grid, kTileThreads, smem, s>>>(ta);
+        const int grid = (int)std::min<long long>(
+            ((long long)(b1 - b0) + kTileWarpsPerCta - 1) / kTileWarpsPerCta, (long long)nsm * occ);
+        kern<<<grid, 32 * kTileWarpsPerCta, smem, s>>>(ta);
         launches++;
         tile_launches++;
         KD_LAUNCH_CHECK("k_tiles");
@@ -706,7 +867,7 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
         stats->edge_pairs = (long long)hs[4];
         stats->warp_tiles = (long long)hs[5];
         stats->entries = total;
-        stats->ms_traverse = ms_trav + 0.0;
+        stats->ms_traverse = ms_trav;
         stats->ms_tiles = ms_tiles;
         stats->ms_total = elapsed(ev.e[0], ev.e[4]);
         stats->tile_launches = tile_launches;

@@ -9,7 +9,8 @@
  *     each) ordered leaf by leaf along the top D levels of that same tree, with
  *     per-node bounding boxes, raw counts and single-field summaries, split
  *     into "runs" (<= KD_RUN_MAX consecutive points of one tree-side field) and
- *     "blocks" (<= KD_BLOCK_MAX consecutive points, the query side of a tile).
+ *     "blocks" (<= KD_BLOCK_MAX consecutive points of one 16-leaf subtree,
+ *     the query side of a tile).
  *
  * Every raw point carries two field ids: qf, its own field (what the
  * reference's query side reads, kdquery.c:67-70), and tf, the low 8 bits of
@@ -31,8 +32,8 @@ extern "C" {
 #endif
 
 #define KD_RUN_MAX 64      /* points per tree-side run (shared-memory tile) */
-#define KD_BLOCK_MAX 256   /* query points per block (one CTA, 8 warps) */
-#define KD_WARPS 8         /* warps per query block */
+#define KD_BLOCK_MAX 128   /* query points per block (one warp, 4 per lane) */
+#define KD_QPL 4           /* query points per lane */
 #define KD_LEAF_TARGET 64  /* unique points per counting leaf, upper bound */
 #define KD_MAX_EDGES 64    /* distinct finite squared edges per count job */
 
@@ -91,7 +92,6 @@ typedef struct kd_catalog {
     int *d_blk_start, *d_blk_len;
     int *d_blk_qf;     /* single own field of the block, -1 when mixed */
     double *d_blk_box; /* 6 per block */
-    double *d_blk_wbox;/* KD_WARPS*6 per block: box of each warp's 32 points */
 
     size_t device_bytes;
 } kd_catalog;
