@@ -1,10 +1,12 @@
 """corruscant_b200: B200-native pair counting behind corruscant's API.
 
-Mirrors the reference package layout (corruscant/__init__.py:1-20): the
-native libraries are loaded from ``bin/`` and the user API lives in
-``clustering`` (trees, auto/cross correlation drivers, estimators) and
-``twopoint.threedim`` / ``twopoint.angular``.
+Mirrors the reference package (corruscant/__init__.py:1-20): the native
+libraries are loaded from ``bin/`` and the user API is ``clustering`` (trees,
+auto/cross-correlation drivers, estimators) and ``twopoint.threedim`` /
+``twopoint.angular``.  Importing the package loads nothing; the libraries are
+opened on first use.
 """
 from ._native import loadlib  # noqa: F401
+from . import clustering, twopoint  # noqa: F401
 
-__all__ = ["clustering", "twopoint"]
+__all__ = ["clustering", "twopoint", "loadlib"]

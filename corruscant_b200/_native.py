@@ -90,12 +90,17 @@ def kdlib():
         L.kd_count_radii.restype = c_int
         L.kd_count_radii.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int,
                                      POINTER(c_longlong), POINTER(CountStats)]
+        L.kd_count_radii_shard.restype = c_int
+        L.kd_count_radii_shard.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int, c_int,
+                                           c_int, POINTER(c_longlong), POINTER(CountStats)]
         L.kd_count_points.restype = c_int
         L.kd_count_points.argtypes = [KdTree, POINTER(c_double), POINTER(c_int), c_int, c_int,
                                       POINTER(c_double), c_int, c_int, POINTER(c_longlong),
                                       POINTER(CountStats)]
         L.kd_tree_permutation.restype = c_int
         L.kd_tree_permutation.argtypes = [KdTree, POINTER(c_int)]
+        L.kd_set_device.restype = c_int
+        L.kd_set_device.argtypes = [c_int]
         L.kd_tree_input_size.restype = c_int
         L.kd_tree_input_size.argtypes = [KdTree]
         _KD = L
@@ -156,6 +161,19 @@ def count_radii(tree, query, radii, mode=KD_MODE_MIXED, with_stats=False):
     return (out, st.as_dict()) if with_stats else out
 
 
+def count_radii_shard(tree, query, radii, shard, nshards, mode=KD_MODE_MIXED, with_stats=False):
+    """One shard of count_radii (query blocks split evenly over nshards)."""
+    radii = np.require(np.asarray(radii, dtype=np.float64), requirements="AC")
+    out = np.zeros((len(radii), query.num_fields * tree.num_fields), dtype=np.int64)
+    st = CountStats()
+    rc = kdlib().kd_count_radii_shard(tree, query, dptr(radii), c_int(len(radii)), c_int(mode),
+                                      c_int(shard), c_int(nshards),
+                                      out.ctypes.data_as(POINTER(c_longlong)), ctypes.byref(st))
+    if rc != 0:
+        raise_last()
+    return (out, st.as_dict()) if with_stats else out
+
+
 def count_points(tree, points, fields, num_fields, radii, mode=KD_MODE_MIXED, with_stats=False):
     points = np.require(points, dtype=np.float64, requirements="AC")
     fields = None if fields is None else np.require(fields, dtype=np.int32, requirements="AC")
@@ -191,5 +209,29 @@ def permutation(tree):
     return perm
 
 
+def set_device(device):
+    """Device used by later tree builds of this thread (kd_set_device)."""
+    if kdlib().kd_set_device(c_int(device)) != 0:
+        raise_last()
+
+
 def destroy(tree):
     kdlib().destroy(tree)
+
+
+_CO = None
+
+
+def coordlib():
+    """bin/libcoords.so with the reference's signatures (coordmath.c:38-80)."""
+    global _CO
+    if _CO is None:
+        L = loadlib("libcoords")
+        L.radec2cart64.restype = None
+        L.radec2cart64.argtypes = [POINTER(c_double)] * 3 + [c_int]
+        L.radecdist2cart64.restype = None
+        L.radecdist2cart64.argtypes = [POINTER(c_double)] * 4 + [c_int]
+        L.radec2sph64.restype = None
+        L.radec2sph64.argtypes = [POINTER(c_double)] * 4 + [c_int]
+        _CO = L
+    return _CO

@@ -148,6 +148,12 @@ int kd_tree_permutation(kdtree_t t, int *perm)
     return kdg_copy_inorder(&h->cat, perm);
 }
 
+int kd_set_device(int device)
+{
+    clear_error();
+    return kdg_set_device(device);
+}
+
 int kd_tree_input_size(kdtree_t t)
 {
     kd_handle *h = lookup(&t);
@@ -168,8 +174,8 @@ static int cmp_double(const void *a, const void *b)
  * (kdquery.c:34: rows strided by the QUERY field count Fq).
  */
 static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, int Fq,
-                          const double *radii, int nradii, int mode, long long *out,
-                          kd_count_stats *stats)
+                          const double *radii, int nradii, int mode, int shard, int nshards,
+                          long long *out, kd_count_stats *stats)
 {
     double *rsq = NULL, *uniq = NULL;
     long long *hist = NULL;
@@ -234,7 +240,7 @@ static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, in
             rc = KD_ENOMEM;
             goto done;
         }
-        rc = kdg_count(tc, qc, uniq, ne, mode, hist, stats);
+        rc = kdg_count(tc, qc, uniq, ne, mode, shard, nshards, hist, stats);
         if (rc != KD_OK) goto done;
         /* cumulative over sorted edges: pairs with d2 < uniq[e] */
         for (k = 1; k < ne; k++) {
@@ -336,13 +342,14 @@ int kd_count_points(kdtree_t tree, const double *xyz, const int *fields, int len
         if (stats) memset(stats, 0, sizeof *stats);
         return KD_OK;
     }
-    rc = count_catalogs(&h->cat, tree.num_fields, &qc, num_fields, radii, nradii, mode, out, stats);
+    rc = count_catalogs(&h->cat, tree.num_fields, &qc, num_fields, radii, nradii, mode, 0, 1, out,
+                        stats);
     kdg_free(&qc);
     return rc;
 }
 
-int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradii, int mode,
-                   long long *out, kd_count_stats *stats)
+int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii, int nradii,
+                         int mode, int shard, int nshards, long long *out, kd_count_stats *stats)
 {
     kd_handle *ht, *hq;
     clear_error();
@@ -350,8 +357,18 @@ int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradi
     if (!ht) return KD_EINVAL;
     hq = lookup_or_fail(&query, "kd_count_radii (query)");
     if (!hq) return KD_EINVAL;
+    if (nshards < 1 || shard < 0 || shard >= nshards) {
+        kd_set_error(KD_EINVAL, "kd_count_radii_shard: shard %d of %d", shard, nshards);
+        return KD_EINVAL;
+    }
     return count_catalogs(&ht->cat, tree.num_fields, &hq->cat, query.num_fields, radii, nradii,
-                          mode, out, stats);
+                          mode, shard, nshards, out, stats);
+}
+
+int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradii, int mode,
+                   long long *out, kd_count_stats *stats)
+{
+    return kd_count_radii_shard(tree, query, radii, nradii, mode, 0, 1, out, stats);
 }
 
 long long *pair_count(kdtree_t tree, double *data, int *fields, int length, int num_fields,

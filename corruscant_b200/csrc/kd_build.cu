@@ -1383,8 +1383,21 @@ extern "C" int kdg_build(const double *h_xyz, const int *h_fields, int n, int nu
     }
 }
 
+// Runs a catalog operation on the catalog's device, then restores the
+// calling thread's device.
+struct OnDevice {
+    int prev = 0;
+    explicit OnDevice(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~OnDevice() { cudaSetDevice(prev); }
+};
+
 extern "C" int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
 {
+    OnDevice on(cat->device);
     if (!cat->d_nodes) {
         kd_set_error(KD_EINVAL, "node array no longer held on the device");
         return KD_EINVAL;
@@ -1400,12 +1413,14 @@ extern "C" int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
 
 extern "C" void kdg_drop_nodes(kd_catalog *cat)
 {
+    OnDevice on(cat->device);
     if (cat->d_nodes) cudaFree(cat->d_nodes);
     cat->d_nodes = nullptr;
 }
 
 extern "C" int kdg_copy_inorder(const kd_catalog *cat, int *h_perm)
 {
+    OnDevice on(cat->device);
     cudaError_t e = cudaMemcpy(h_perm, cat->d_inorder_rep, sizeof(int) * (size_t)cat->n_u,
                                cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
@@ -1417,6 +1432,7 @@ extern "C" int kdg_copy_inorder(const kd_catalog *cat, int *h_perm)
 
 extern "C" void kdg_free(kd_catalog *cat)
 {
+    OnDevice on(cat->device);
     void *ptrs[] = {cat->d_nodes,    cat->d_inorder_rep, cat->d_x,       cat->d_y,
                     cat->d_z,        cat->d_qf,          cat->fields_split ? cat->d_tf : nullptr,
                     cat->d_box,      cat->d_ncount,      cat->d_ntf,     cat->d_nqf,

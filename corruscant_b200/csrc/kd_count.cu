@@ -706,8 +706,10 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b)
 }
 
 static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double *h_rsq, int ne,
-                       int mode, long long *hist, kd_count_stats *stats)
+                       int mode, int shard, int nshards, long long *hist, kd_count_stats *stats)
 {
+    if (tc->device != qc->device) raise(KD_EINVAL, "tree and query catalogs on different devices");
+    check(cudaSetDevice(tc->device), "cudaSetDevice");
     init_device();
     Stream st;
     cudaStream_t s = st.s;
@@ -751,8 +753,14 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     check(cudaMemsetAsync(err, 0, sizeof(int), s), "memset");
     check(cudaMemcpyAsync(rsq, h_rsq, sizeof(double) * ne, cudaMemcpyHostToDevice, s), "H2D");
 
-    const int nb = qc->nblocks;
-    int *cnt = pool.alloc<int>(nb);
+    // this shard's query blocks, renumbered from 0
+    const int blo = (int)((long long)qc->nblocks * shard / nshards);
+    const int nb = (int)((long long)qc->nblocks * (shard + 1) / nshards) - blo;
+    Q.blk_start += blo;
+    Q.blk_len += blo;
+    Q.blk_qf += blo;
+    Q.blk_box += 6 * (size_t)blo;
+    int *cnt = pool.alloc<int>(std::max(nb, 1));
     TravOut to;
     memset(&to, 0, sizeof to);
     to.count = cnt;
@@ -761,8 +769,10 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     to.Fte = Fte;
     to.accepted = dstats + 2;
     to.err = err;
-    k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0, nb, to);
-    launches++;
+    if (nb > 0) {
+        k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0, nb, to);
+        launches++;
+    }
     KD_LAUNCH_CHECK("k_traverse(count)");
     std::vector<int> hcnt(nb);
     check(cudaMemcpyAsync(hcnt.data(), cnt, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToHost, s),
@@ -877,15 +887,36 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
 
 }  // namespace kd
 
-extern "C" int kdg_count(const kd_catalog *tree, const kd_catalog *query, const double *rsq,
-                         int ne, int mode, long long *hist, kd_count_stats *stats)
+extern "C" int kdg_set_device(int device)
 {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        kd_set_error(KD_ENODEV, "no CUDA device %d (%d visible)", device, n);
+        return KD_ENODEV;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        kd_set_error(KD_ECUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+        return KD_ECUDA;
+    }
+    return KD_OK;
+}
+
+extern "C" int kdg_count(const kd_catalog *tree, const kd_catalog *query, const double *rsq,
+                         int ne, int mode, int shard, int nshards, long long *hist,
+                         kd_count_stats *stats)
+{
+    if (nshards < 1 || shard < 0 || shard >= nshards) {
+        kd_set_error(KD_EINVAL, "shard %d of %d", shard, nshards);
+        return KD_EINVAL;
+    }
     if (ne < 1 || ne > KD_MAX_EDGES) {
         kd_set_error(KD_EINVAL, "between 1 and %d distinct radii per count", KD_MAX_EDGES);
         return KD_EINVAL;
     }
     try {
-        kd::count_impl(tree, query, rsq, ne, mode, hist, stats);
+        kd::count_impl(tree, query, rsq, ne, mode, shard, nshards, hist, stats);
         return KD_OK;
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);

@@ -117,14 +117,19 @@ void kdg_free(kd_catalog *cat);
  *              hist[e][qf][tf] = pairs whose FP64 squared distance d2
  *              satisfies rsq[e-1] <= d2 < rsq[e] (e = ne: beyond all edges,
  *              left zero)
+ *   shard, nshards: count only query blocks [nb*shard/nshards,
+ *              nb*(shard+1)/nshards) of the query catalog's nb blocks
  */
 int kdg_count(const kd_catalog *tree, const kd_catalog *query,
-              const double *rsq, int ne, int mode, long long *hist,
-              kd_count_stats *stats);
+              const double *rsq, int ne, int mode, int shard, int nshards,
+              long long *hist, kd_count_stats *stats);
 
 /* Coordinates (libcoords). */
 int kdg_radec2cart(const double *ra, const double *dec, const double *dist,
                    double *xyz, int n);
+
+/* cudaSetDevice for the calling thread, with the library's error reporting */
+int kdg_set_device(int device);
 
 void kd_set_error(int code, const char *fmt, ...);
 

@@ -126,6 +126,15 @@ void kd_free_counts(long long *counts);
 int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii,
                    int nradii, int mode, long long *out, kd_count_stats *stats);
 
+/* One shard of kd_count_radii: only the query points of query blocks
+ * [nb*shard/nshards, nb*(shard+1)/nshards) are counted (nb: the query
+ * tree's blocks of up to 128 spatially adjacent points).  Summing out over
+ * all shards gives kd_count_radii's result exactly; one shard per GPU splits
+ * a count across devices with no exchange until that final sum. */
+int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii,
+                         int nradii, int mode, int shard, int nshards,
+                         long long *out, kd_count_stats *stats);
+
 /* Same, with arbitrary query points (interleaved xyz, fields may be NULL). */
 int kd_count_points(kdtree_t tree, const double *xyz, const int *fields,
                     int length, int num_fields, const double *radii,
@@ -136,6 +145,12 @@ int kd_count_points(kdtree_t tree, const double *xyz, const int *fields,
  * given to tree_construct, of the (first occurrence of the) point stored at
  * in-order position i.  perm holds tree.size ints. */
 int kd_tree_permutation(kdtree_t tree, int *perm);
+
+/* Selects the CUDA device used by later tree_construct calls of the calling
+ * thread (default 0; the library has its own CUDA runtime, so a device
+ * selected through another library does not apply).  Counts always run on
+ * the device holding their trees.  Returns 0 or a negative error code. */
+int kd_set_device(int device);
 
 /* Raw (input) point count of a tree, duplicates included. */
 int kd_tree_input_size(kdtree_t tree);

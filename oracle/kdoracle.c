@@ -549,6 +549,68 @@ int or_brute_counts(const or_tree_t *t, const double *q, const int *qfields,
     return OR_OK;
 }
 
+/* ------------------------------------------------------------ visit count */
+
+typedef struct {
+    const double *nxyz;
+    const int *has_l, *has_r, *dim;
+    const double *q;
+    int lo, hi;
+    double r;
+    long long visits;
+} visit_t;
+
+static void visit_rec(visit_t *v, int p, const double *q)
+{
+    v->visits++;
+    if (!v->has_l[p]) return;
+    if (!v->has_r[p]) {
+        visit_rec(v, 2 * p, q);
+        return;
+    }
+    int d = v->dim[p];
+    double val = q[d], point = v->nxyz[3 * (size_t)p + d];
+    if (val + v->r < point) visit_rec(v, 2 * p, q);
+    else if (val - v->r > point) visit_rec(v, 2 * p + 1, q);
+    else {
+        visit_rec(v, 2 * p, q);
+        visit_rec(v, 2 * p + 1, q);
+    }
+}
+
+static void *visit_worker(void *arg)
+{
+    visit_t *v = (visit_t *)arg;
+    for (int i = v->lo; i < v->hi; i++) visit_rec(v, 1, v->q + 3 * (size_t)i);
+    return NULL;
+}
+
+long long or_count_visits(const double *nxyz, const int *has_l, const int *has_r,
+                          const int *dim, int memsize, const double *q, int nq,
+                          double r, int nthreads)
+{
+    (void)memsize;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 64) nthreads = 64;
+    visit_t vs[64];
+    pthread_t th[64];
+    for (int i = 0; i < nthreads; i++) {
+        vs[i] = (visit_t){nxyz, has_l, has_r, dim, q,
+                          (int)((long long)nq * i / nthreads),
+                          (int)((long long)nq * (i + 1) / nthreads), r, 0};
+    }
+    int started[64] = {0};
+    for (int i = 1; i < nthreads; i++) started[i] = pthread_create(&th[i], NULL, visit_worker, &vs[i]) == 0;
+    visit_worker(&vs[0]);
+    long long tot = vs[0].visits;
+    for (int i = 1; i < nthreads; i++) {
+        if (started[i]) pthread_join(th[i], NULL);
+        else visit_worker(&vs[i]);
+        tot += vs[i].visits;
+    }
+    return tot;
+}
+
 /* ------------------------------------------------------------- coordinates */
 
 #define OR_DEG2RAD (M_PI / 180.0) /* PI_OVER_180, coordmath.c:20 */

@@ -68,6 +68,14 @@ int or_brute_counts(const or_tree_t *t, const double *q, const int *qfields,
                     int nq, int num_fields_q, const double *radii, int nradii,
                     int nthreads, long long *out);
 
+/* Node distance evaluations the reference traversal (kdquery.c:62-113)
+ * performs for nq queries at radius r, over a node array given by its
+ * semantic fields (memsize entries; xyz interleaved).  This is the CPU
+ * path's "pairs tested" count. */
+long long or_count_visits(const double *nxyz, const int *has_l, const int *has_r,
+                          const int *dim, int memsize, const double *q, int nq,
+                          double r, int nthreads);
+
 void or_radec2cart64(const double *ra, const double *dec, double *xyz, int n);
 void or_radecdist2cart64(const double *ra, const double *dec,
                          const double *dist, double *xyz, int n);

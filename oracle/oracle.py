@@ -52,6 +52,9 @@ def lib():
         L.or_brute_counts.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int), c_int,
                                       c_int, POINTER(c_double), c_int, c_int,
                                       POINTER(c_longlong)]
+        L.or_count_visits.restype = c_longlong
+        L.or_count_visits.argtypes = [POINTER(c_double)] + [POINTER(c_int)] * 3 + [
+            c_int, POINTER(c_double), c_int, c_double, c_int]
         for f in ("or_radec2cart64",):
             getattr(L, f).argtypes = [POINTER(c_double)] * 3 + [c_int]
         L.or_radecdist2cart64.argtypes = [POINTER(c_double)] * 4 + [c_int]
@@ -135,6 +138,17 @@ class OracleTree:
         if rc != 0:
             raise OracleError(lib().or_last_error().decode())
         return out
+
+
+def count_visits(nodes, q, r, nthreads=8):
+    """Reference traversal node visits (its "pairs tested") over a node array
+    given as the dict returned by OracleTree.nodes() / RefLib.nodes()."""
+    xyz = np.require(nodes["xyz"], dtype=np.float64, requirements="AC")
+    hl, hr, dm = (np.require(nodes[k], dtype=np.int32, requirements="AC")
+                  for k in ("has_l", "has_r", "dim"))
+    q = np.require(q, dtype=np.float64, requirements="AC")
+    return lib().or_count_visits(_dp(xyz), _ip(hl), _ip(hr), _ip(dm), c_int(len(hl)), _dp(q),
+                                 c_int(q.shape[0]), c_double(r), c_int(nthreads))
 
 
 def radec2cart64(ra, dec):

@@ -1,0 +1,76 @@
+"""The user API end to end on the GPU (tree build, batched counts, estimators)
+against the reference's golden outputs and the oracle."""
+import numpy as np
+import pytest
+
+from corruscant_b200 import _native, clustering, twopoint
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.asarray(a, dtype=np.float64).view(np.int64)
+
+
+@pytest.mark.parametrize("mode", [_native.KD_MODE_MIXED, _native.KD_MODE_FP64])
+def test_example_autocorr_end_to_end(golden, mode):
+    """The reference's test/example.py workload through twopoint.threedim."""
+    g = golden("config1.npz")
+    np.random.seed(3)
+    X = np.random.rand(4000, 3)
+    Y = np.random.rand(80000, 3)
+    dtree = clustering.tree(X, (X[:, 0] * 4).astype("int32"))
+    rtree = clustering.tree(Y, (Y[:, 0] * 4).astype("int32"))
+    res = twopoint.threedim.autocorr(dtree, rtree, np.logspace(-2.5, -1., 6),
+                                     est_type="landy-szalay", num_threads=4, mode=mode)
+    for k in ("dd", "dr", "rr"):
+        assert np.array_equal(getattr(res, k), g[k]), k
+    assert np.array_equal(_bits(res.estimate()), _bits(g["xi"]))
+    assert np.array_equal(_bits(res.error("jackknife")), _bits(g["err_jackknife"]))
+    res.error_type = "jackknife"
+    assert "Estimator" in str(res)
+
+
+def test_crosscorr_end_to_end(golden):
+    g = golden("cross.npz")
+    rs = np.random.RandomState(int(g["seed"]))
+    cats = [rs.rand(int(n), 3) for n in g["sizes"]]
+    trees = [clustering.tree(c, (c[:, 0] * 4).astype("int32")) for c in cats]
+    res = twopoint.threedim.crosscorr(*trees, g["radii"])
+    for k in ("d1d2", "d1r2", "d2r1", "r1r2"):
+        assert np.array_equal(getattr(res, k), g[k]), k
+    assert np.array_equal(_bits(res.estimate()), _bits(g["xi"]))
+    assert np.array_equal(_bits(res.error("jackknife")), _bits(g["err_jackknife"]))
+
+
+def test_reference_query_tree_entry_point_matches():
+    """_query_tree goes through pair_count, one radius at a time, like the
+    reference driver; it must agree with the batched counts."""
+    rs = np.random.RandomState(2)
+    X = rs.rand(3000, 3)
+    f = (X[:, 1] * 3).astype("int32")
+    t = clustering.tree(X, f)
+    radii = np.array([0.01, 0.03, 0.08])
+    batched = _native.count_radii(t.ctree, t.ctree, radii).reshape(3, 3, 3)
+    for k, r in enumerate(radii):
+        assert np.array_equal(clustering._query_tree(t, t.points, r, 4, t.fields, 3), batched[k])
+
+
+def test_angular_autocorr_matches_oracle():
+    rs = np.random.RandomState(4)
+    n, m = 3000, 20000
+    ra_d, ra_r = rs.rand(n) * 90, rs.rand(m) * 90
+    dec_d = np.degrees(np.arcsin(rs.uniform(np.sin(np.radians(-10)), np.sin(np.radians(60)), n)))
+    dec_r = np.degrees(np.arcsin(rs.uniform(np.sin(np.radians(-10)), np.sin(np.radians(60)), m)))
+    Xd, Xr = twopoint.angular.cartesian(ra_d, dec_d), twopoint.angular.cartesian(ra_r, dec_r)
+    fd, fr = (ra_d / 30).astype("int32"), (ra_r / 30).astype("int32")
+    deg = np.logspace(-1, np.log10(5.0), 6)
+    res = twopoint.angular.autocorr(clustering.tree(Xd, fd), clustering.tree(Xr, fr), deg)
+    chords = twopoint.angular.chord(deg)
+    od, orr = O.OracleTree(Xd, fd, 3), O.OracleTree(Xr, fr, 3)
+    dd = np.diff(od.brute_counts(Xd, fd, 3, chords, nthreads=8), axis=0).reshape(-1, 3, 3)
+    rr = np.diff(orr.brute_counts(Xr, fr, 3, chords, nthreads=8), axis=0).reshape(-1, 3, 3)
+    assert np.array_equal(res.dd, dd)
+    assert np.array_equal(res.rr, rr)
+    assert res.radii_units == "degrees"

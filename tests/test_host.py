@@ -1,0 +1,122 @@
+"""Host-side checks that need no GPU: the C ABI libraries load and export what
+include/*.h declares, the estimator/error/covariance arithmetic matches the
+reference's own outputs to 0 ulp, input validation behaves like the
+reference, and the coordinate conversions are bit-identical."""
+import ctypes
+import os
+import re
+import types
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+from corruscant_b200 import _native, clustering, twopoint
+
+
+def _declared(header):
+    """Function names declared in a C header (prototype lines)."""
+    src = open(os.path.join(REPO, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("if", "while", "sizeof")))
+
+
+@pytest.mark.parametrize("lib,header", [("libkdtree", "kdtree.h"), ("libcoords", "coordmath.h")])
+def test_library_exports_every_declared_symbol(lib, header):
+    names = _declared(header)
+    assert names, header
+    L = ctypes.CDLL(os.path.join(REPO, "corruscant_b200", "bin", lib + ".so"))
+    for name in names:
+        assert hasattr(L, name), (lib, name)
+
+
+def test_reference_abi_struct_sizes():
+    assert ctypes.sizeof(_native.KdTree) == 64
+    assert ctypes.sizeof(_native.Node) == 40
+    assert ctypes.sizeof(_native.Datum) == 32
+
+
+def _fake_tree(fields, n_fields):
+    return types.SimpleNamespace(N_fields=n_fields,
+                                 field_sizes=np.array([np.sum(fields == i) for i in range(n_fields)]))
+
+
+def _assert_bits(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    assert a.shape == b.shape
+    assert np.array_equal(a.view(np.int64), b.view(np.int64)), (a, b)
+
+
+def _check_estimators(res, g):
+    _assert_bits(res.estimate(), g["xi"])
+    _assert_bits(res.error("jackknife"), g["err_jackknife"])
+    _assert_bits(res.error("ftf"), g["err_ftf"])
+    _assert_bits(res.error("poisson"), g["err_poisson"])
+    _assert_bits(res.covariance("jackknife"), g["cov_jackknife"])
+    _assert_bits(res.covariance("jackknife", normalized=True), g["cov_jackknife_norm"])
+    _assert_bits(res.covariance("ftf"), g["cov_ftf"])
+    np.random.seed(11)
+    _assert_bits(res.error("bootstrap"), g["err_bootstrap_seed11"])
+
+
+def test_autocorr_estimators_match_reference_to_0ulp(golden):
+    g = golden("config1.npz")
+    np.random.seed(3)
+    X = np.random.rand(4000, 3)
+    Y = np.random.rand(80000, 3)
+    fd = (X[:, 0] * 4).astype("int32")
+    fr = (Y[:, 0] * 4).astype("int32")
+    res = clustering.autocorr_results(g["dd"], g["dr"], g["rr"], _fake_tree(fd, 4),
+                                      _fake_tree(fr, 4), clustering.est_landy_szalay, g["radii"])
+    _check_estimators(res, g)
+    for est in ("standard", "hamilton"):
+        res.estimator = getattr(clustering, "est_" + est)
+        _assert_bits(res.estimate(), g["xi_" + est])
+        _assert_bits(res.error("jackknife"), g["err_jackknife_" + est])
+
+
+def test_crosscorr_estimators_match_reference_to_0ulp(golden):
+    g = golden("cross.npz")
+    rs = np.random.RandomState(int(g["seed"]))
+    cats = [rs.rand(int(n), 3) for n in g["sizes"]]
+    fakes = [_fake_tree((c[:, 0] * 4).astype("int32"), 4) for c in cats]
+    res = clustering.crosscorr_results(g["d1d2"], g["d1r2"], g["d2r1"], g["r1r2"], *fakes,
+                                       clustering.est_landy_szalay, g["radii"])
+    _check_estimators(res, g)
+
+
+def test_results_table_prints():
+    dd = np.arange(1, 9).reshape(2, 2, 2)
+    res = clustering.autocorr_results(dd, dd + 1, dd + 2, _fake_tree(np.array([0, 1]), 2),
+                                      _fake_tree(np.array([0, 1]), 2),
+                                      clustering.est_landy_szalay, np.array([0.1, 0.2, 0.3]))
+    res.radii_nominal = res.radii_euclidean
+    res.radii_units = "Data units"
+    res.error_type = "jackknife"
+    text = str(res)
+    assert "Bin L" in text and "Estimator" in text and len(text.splitlines()) == 7
+
+
+def test_validation_like_reference():
+    with pytest.raises(ValueError):
+        clustering.validate_points(np.zeros((5, 4)))
+    with pytest.warns(RuntimeWarning):
+        p = clustering.validate_points(np.zeros((3, 10)))
+    assert p.shape == (10, 3)
+    with pytest.raises(ValueError):
+        clustering.validate_fields(np.zeros(9), p)
+    assert clustering.validate_fields(np.zeros(10), p).dtype == np.int32
+    with pytest.raises(ValueError):
+        clustering._estimator("no-such-estimator")
+
+
+def test_coordinates_bit_identical_to_reference(golden):
+    c = golden("coords.npz")
+    _assert_bits(twopoint.angular.cartesian(c["ra"], c["dec"]), c["xyz"])
+    _assert_bits(twopoint.threedim.cartesian(c["ra"], c["dec"], c["dist"]), c["xyzd"])
+
+
+def test_chord_edges_are_the_reference_expression():
+    deg = np.logspace(-3, np.log10(2.0), 16)
+    _assert_bits(twopoint.angular.chord(deg), 2. * np.sin(deg * (np.pi / 180.) / 2.))
