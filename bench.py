@@ -153,21 +153,29 @@ def fp32_peak_tflops(device):
         return None
 
 
+def shard_range(n, shard, nshards):
+    """[lo, hi) of shard `shard` of n items split evenly over nshards, the
+    split kd_count_radii_shard applies to query blocks."""
+    return n * shard // nshards, n * (shard + 1) // nshards
+
+
 class Dist:
     """torch.distributed plumbing (barrier, sum/max reductions) when WORLD_SIZE > 1."""
 
-    def __init__(self):
+    def __init__(self, backend="nccl"):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.dist = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.dist, self.torch = dist, torch
 
     def barrier(self):
@@ -177,7 +185,8 @@ class Dist:
     def reduce(self, arr, op):
         if not self.dist:
             return np.asarray(arr)
-        t = self.torch.tensor(np.asarray(arr), device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor(np.asarray(arr), device=dev)
         self.dist.all_reduce(t, op=getattr(self.dist.ReduceOp, op))
         return t.cpu().numpy()
 

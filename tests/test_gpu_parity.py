@@ -183,3 +183,20 @@ def test_errors_are_reported_not_fatal():
         assert np.array_equal(got, want)
     finally:
         N.destroy(t)
+
+
+def test_shards_sum_to_full_count():
+    """kd_count_radii_shard: the shards of the query blocks partition the
+    count exactly (the multi-GPU split, run here on one device)."""
+    rs = np.random.RandomState(17)
+    p = _clustered(rs, 40000, 200, 0.01)
+    f = (p[:, 2] * 4).astype(np.int32)
+    t = _tree(p, f, 4)
+    radii = np.logspace(-2.5, -1, 7)
+    try:
+        full = N.count_radii(t, t, radii)
+        for nshards in (2, 3, 8):
+            parts = [N.count_radii_shard(t, t, radii, s, nshards) for s in range(nshards)]
+            assert np.array_equal(sum(parts), full), nshards
+    finally:
+        N.destroy(t)
