@@ -93,6 +93,9 @@ def kdlib():
         L.kd_count_radii_shard.restype = c_int
         L.kd_count_radii_shard.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int, c_int,
                                            c_int, POINTER(c_longlong), POINTER(CountStats)]
+        L.kd_count_radii_static.restype = c_int
+        L.kd_count_radii_static.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int,
+                                            POINTER(c_longlong)]
         L.kd_count_points.restype = c_int
         L.kd_count_points.argtypes = [KdTree, POINTER(c_double), POINTER(c_int), c_int, c_int,
                                       POINTER(c_double), c_int, c_int, POINTER(c_longlong),
@@ -172,6 +175,17 @@ def count_radii_shard(tree, query, radii, shard, nshards, mode=KD_MODE_MIXED, wi
     if rc != 0:
         raise_last()
     return (out, st.as_dict()) if with_stats else out
+
+
+def count_radii_static(tree, query, radii, mode=KD_MODE_MIXED):
+    """count_radii through kd_count_radii_static (no allocation in the call)."""
+    radii = np.require(np.asarray(radii, dtype=np.float64), requirements="AC")
+    out = np.zeros((len(radii), query.num_fields * tree.num_fields), dtype=np.int64)
+    rc = kdlib().kd_count_radii_static(tree, query, dptr(radii), c_int(len(radii)), c_int(mode),
+                                       out.ctypes.data_as(POINTER(c_longlong)))
+    if rc != 0:
+        raise_last()
+    return out
 
 
 def count_points(tree, points, fields, num_fields, radii, mode=KD_MODE_MIXED, with_stats=False):

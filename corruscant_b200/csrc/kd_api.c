@@ -371,6 +371,62 @@ int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradi
     return kd_count_radii_shard(tree, query, radii, nradii, mode, 0, 1, out, stats);
 }
 
+int kd_count_radii_static(kdtree_t tree, kdtree_t query, const double *radii, int nradii,
+                          int mode, long long *out)
+{
+    /* no heap: the radii are sorted in fixed arrays (insertion sort) */
+    double uniq[KD_MAX_EDGES];
+    int edge_of[KD_MAX_EDGES];
+    int k, j, ne = 0;
+    kd_handle *ht, *hq;
+    clear_error();
+    ht = lookup_or_fail(&tree, "kd_count_radii_static (tree)");
+    if (!ht) return KD_EINVAL;
+    hq = lookup_or_fail(&query, "kd_count_radii_static (query)");
+    if (!hq) return KD_EINVAL;
+    if (nradii < 0 || nradii > KD_MAX_EDGES || (nradii > 0 && (!radii || !out))) {
+        kd_set_error(KD_EINVAL, "kd_count_radii_static: 0 to %d radii and an output array",
+                     KD_MAX_EDGES);
+        return KD_EINVAL;
+    }
+    if (mode != KD_MODE_MIXED && mode != KD_MODE_FP64) {
+        kd_set_error(KD_EINVAL, "unknown count mode %d", mode);
+        return KD_EINVAL;
+    }
+    if (query.num_fields < 1 || tree.num_fields < 1 || hq->cat.min_qf < 0 ||
+        (long long)hq->cat.max_qf * query.num_fields + ht->cat.max_tf >=
+            (long long)query.num_fields * tree.num_fields) {
+        kd_set_error(KD_EFIELD, "field ids overflow the %d x %d counter (qfield*%d + tfield)",
+                     query.num_fields, tree.num_fields, query.num_fields);
+        return KD_EFIELD;
+    }
+    for (k = 0; k < nradii; k++) {
+        double v = radii[k] * radii[k]; /* kdquery.c:77 */
+        if (radii[k] < 0) {
+            kd_set_error(KD_ERADIUS, "negative radius %g", radii[k]);
+            return KD_ERADIUS;
+        }
+        if (v != v) continue;
+        for (j = 0; j < ne && uniq[j] != v; j++)
+            ;
+        if (j < ne) continue;
+        for (j = ne++; j > 0 && uniq[j - 1] > v; j--) uniq[j] = uniq[j - 1];
+        uniq[j] = v;
+    }
+    for (k = 0; k < nradii; k++) {
+        double v = radii[k] * radii[k];
+        edge_of[k] = -1;
+        for (j = 0; j < ne; j++)
+            if (uniq[j] == v) edge_of[k] = j;
+    }
+    if (ne == 0) {
+        memset(out, 0, sizeof(long long) * (size_t)nradii * query.num_fields * tree.num_fields);
+        return KD_OK;
+    }
+    return kdg_count_static(&ht->cat, tree.num_fields, &hq->cat, query.num_fields, uniq, ne,
+                            edge_of, nradii, mode, out);
+}
+
 long long *pair_count(kdtree_t tree, double *data, int *fields, int length, int num_fields,
                       double r, int num_threads)
 {

@@ -33,6 +33,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "kd_cuda_util.cuh"
@@ -885,7 +886,259 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     }
 }
 
+// ------------------------------------------------------------------------
+// Count without any allocation (kd_count_radii_static).
+//
+// For callers that cannot allocate device memory at count time: every
+// per-call buffer of a count (bin histogram, tile records, block offsets,
+// scan workspace, counters, the final per-radius matrices) is carved out of
+// one file-scope device array.  Every GPU that loads the library holds this
+// array until the process exits.  All calls on a device share it and it keeps
+// the previous call's contents, so everything that must start at zero is
+// cleared at the start of a call, and two calls that overlap on the same GPU
+// race.  Jobs whose tile records do not fit are counted in as many batches as
+// it takes.
+
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void *g_static_ptr[kMaxDevices];  // device address of g_static_scratch, per device
+}  // namespace
+
+// Device address of the scratch array on the current device.  Host code
+// cannot use the symbol itself (on the host it names a host-side stand-in),
+// so the address is looked up once per device with that device current.
+static unsigned char *static_scratch(int device)
+{
+    if (device < 0 || device >= kMaxDevices) raise(KD_ENODEV, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[device]) {
+        void *ptr = nullptr;
+        check(cudaGetSymbolAddress(&ptr, g_static_scratch), "cudaGetSymbolAddress(scratch)");
+        g_static_ptr[device] = ptr;
+    }
+    return (unsigned char *)g_static_ptr[device];
+}
+
+// last block b1 > b0 such that blocks [b0, b1) have at most cap tile records
+// (at least one block); records of block b0 alone above cap: b1 = -1
+__global__ void k_static_batch(const long long *off, int nb, int b0, long long cap, int *b1_out,
+                               long long *rel, int rel_cap)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int lo = b0 + 1, hi = nb;
+        if (off[b0 + 1] - off[b0] > cap) {
+            *b1_out = -1;
+            return;
+        }
+        while (lo < hi) {  // largest b1 in [b0+1, nb] with off[b1] - off[b0] <= cap
+            const int mid = (lo + hi + 1) / 2;
+            if (off[mid] - off[b0] <= cap) lo = mid;
+            else hi = mid - 1;
+        }
+        *b1_out = min(lo, b0 + rel_cap - 1);
+    }
+    __syncthreads();
+    const int b1 = *b1_out;
+    for (int i = threadIdx.x; b1 > b0 && i <= b1 - b0; i += blockDim.x)
+        rel[i] = off[b0 + i] - off[b0];
+}
+
+// hist[e][qf][tf] -> out[k][qf*Fq + tf]: the pairs with d2 < rsq of radius k
+// (cumulative over sorted edges), in the reference's counter layout
+__global__ void k_static_out(const unsigned long long *H, int ne, int Fqe, int Fte,
+                             const int *edge_of, int nradii, int Fq, int Ft, long long *out)
+{
+    const int nrow = Fq * Ft;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nradii * nrow;
+         i += gridDim.x * blockDim.x)
+        out[i] = 0;
+    __syncthreads();
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nradii * Fqe * Fte;
+         i += gridDim.x * blockDim.x) {
+        const int k = i / (Fqe * Fte), qf = (i / Fte) % Fqe, tf = i % Fte;
+        const int e = edge_of[k];
+        if (e < 0) continue;
+        unsigned long long v = 0;
+        for (int j = 0; j <= e; j++) v += H[((size_t)j * Fqe + qf) * Fte + tf];
+        atomicAdd((unsigned long long *)&out[(size_t)k * nrow + qf * Fq + tf], v);
+    }
+}
+
+// int tile counts per block (staged in the offsets' storage) widened to int64
+__global__ void k_gather_widen(const int *in, int n, long long *out)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
+static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc, int Fq,
+                              const double *rsq_sorted, int ne, const int *edge_of, int nradii,
+                              int mode, long long *h_out)
+{
+    if (tc->device != qc->device) raise(KD_EINVAL, "tree and query catalogs on different devices");
+    check(cudaSetDevice(tc->device), "cudaSetDevice");
+    unsigned char *base = static_scratch(tc->device);
+    const cudaStream_t s = 0;  // legacy default stream: nothing is created
+
+    TreeSide T;
+    T.x = tc->d_x;
+    T.y = tc->d_y;
+    T.z = tc->d_z;
+    T.box = tc->d_box;
+    T.count = tc->d_ncount;
+    T.tf = tc->d_ntf;
+    T.leaf_run = tc->d_leaf_run;
+    T.run_start = tc->d_run_start;
+    T.run_len = tc->d_run_len;
+    T.run_tf = tc->d_run_tf;
+    T.D = tc->depth;
+    T.nleaves = tc->nleaves;
+    QuerySide Q;
+    Q.x = qc->d_x;
+    Q.y = qc->d_y;
+    Q.z = qc->d_z;
+    Q.qf = qc->d_qf;
+    Q.blk_start = qc->d_blk_start;
+    Q.blk_len = qc->d_blk_len;
+    Q.blk_qf = qc->d_blk_qf;
+    Q.blk_box = qc->d_blk_box;
+    const int nb = qc->nblocks;
+    const int Fqe = qc->max_qf + 1, Fte = tc->max_tf + 1;
+    const size_t hsz = (size_t)(ne + 1) * Fqe * Fte;
+
+    // carve the scratch
+    size_t at = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char *p = base + at;
+        at = align_up(at + bytes);
+        return p;
+    };
+    auto *H = (unsigned long long *)take(sizeof(unsigned long long) * hsz);
+    auto *misc = (unsigned long long *)take(sizeof(unsigned long long) * 8);  // stats
+    auto *err = (int *)take(sizeof(int) * 4);  // err, work, b1
+    auto *rsq = (double *)take(sizeof(double) * KD_MAX_EDGES);
+    auto *eo = (int *)take(sizeof(int) * KD_MAX_EDGES);
+    auto *out = (long long *)take(sizeof(long long) * (size_t)nradii * Fq * Ft);
+    auto *cnt = (long long *)take(sizeof(long long) * ((size_t)nb + 1));
+    auto *off = (long long *)take(sizeof(long long) * ((size_t)nb + 1));
+    size_t scan_bytes = 0;
+    check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt, off, nb + 1, s), "scan size");
+    void *scan_tmp = take(scan_bytes);
+    const int rel_cap = 4096;  // blocks per batch
+    auto *rel = (long long *)take(sizeof(long long) * (rel_cap + 1));
+    if (at + 16 * 64 > kStaticScratchBytes)
+        raise(KD_EINVAL, "count too large for the static scratch (needs more than 32 MiB for "
+                         "its histogram and block tables)");
+    const long long cap = (long long)((kStaticScratchBytes - at) / sizeof(uint4));
+    auto *rec = (uint4 *)(base + at);
+
+    check(cudaMemsetAsync(H, 0, sizeof(unsigned long long) * hsz, s), "memset");
+    check(cudaMemsetAsync(misc, 0, sizeof(unsigned long long) * 8, s), "memset");
+    check(cudaMemsetAsync(err, 0, sizeof(int) * 4, s), "memset");
+    check(cudaMemsetAsync(cnt, 0, sizeof(long long) * ((size_t)nb + 1), s), "memset");
+    check(cudaMemcpyAsync(rsq, rsq_sorted, sizeof(double) * ne, cudaMemcpyHostToDevice, s), "H2D");
+    check(cudaMemcpyAsync(eo, edge_of, sizeof(int) * nradii, cudaMemcpyHostToDevice, s), "H2D");
+
+    // tile counts per block (the traversal writes int counts; widen in place)
+    TravOut to;
+    memset(&to, 0, sizeof to);
+    to.count = (int *)off;  // int counts, staged in off's storage
+    to.H = H;
+    to.Fqe = Fqe;
+    to.Fte = Fte;
+    to.accepted = misc + 2;
+    to.err = err;
+    if (nb > 0)
+        k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0,
+                                                                                  nb, to);
+    KD_LAUNCH_CHECK("k_traverse(count)");
+    k_gather_widen<<<blocks_for(nb, 256), 256, 0, s>>>((const int *)off, nb, cnt);
+    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cnt, off, nb + 1, s), "scan");
+
+    const size_t smem = tile_smem(ne, mode);
+    auto kern = mode == KD_MODE_MIXED ? k_tiles<KD_MODE_MIXED> : k_tiles<KD_MODE_FP64>;
+    check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+          "smem attribute");
+    int nsm = 148, occ = 1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, tc->device);
+    check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * kTileWarpsPerCta, smem),
+          "occupancy");
+    occ = std::max(occ, 1);
+    int b0 = 0;
+    while (b0 < nb) {
+        k_static_batch<<<1, 256, 0, s>>>(off, nb, b0, cap, err + 2, rel, rel_cap);
+        KD_LAUNCH_CHECK("k_static_batch");
+        int b1 = 0;
+        check(cudaMemcpyAsync(&b1, err + 2, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+        check(cudaStreamSynchronize(s), "sync");
+        if (b1 < 0) raise(KD_EINVAL, "a query block has more tile records than the static scratch holds");
+        TravOut tf = to;
+        tf.count = nullptr;
+        tf.off = rel;
+        tf.rec = rec;
+        k_traverse<true><<<blocks_for(b1 - b0, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne,
+                                                                                      b0, b1, tf);
+        KD_LAUNCH_CHECK("k_traverse(fill)");
+        TileArgs ta;
+        ta.tx = tc->d_x;
+        ta.ty = tc->d_y;
+        ta.tz = tc->d_z;
+        ta.t4 = (const float4 *)tc->d_t4;
+        ta.leaf_c = tc->d_leaf_c;
+        ta.hT = tc->leaf_hdiag * (1.0 + 1e-12);
+        ta.Q = Q;
+        ta.rsq = rsq;
+        ta.ne = ne;
+        ta.b0 = b0;
+        ta.b1 = b1;
+        ta.off = rel;
+        ta.rec = rec;
+        ta.H = H;
+        ta.Fqe = Fqe;
+        ta.Fte = Fte;
+        ta.work = err + 1;
+        ta.stats = misc;
+        check(cudaMemsetAsync(err + 1, 0, sizeof(int), s), "memset");
+        const int grid = (int)std::min<long long>(
+            ((long long)(b1 - b0) + kTileWarpsPerCta - 1) / kTileWarpsPerCta, (long long)nsm * occ);
+        kern<<<grid, 32 * kTileWarpsPerCta, smem, s>>>(ta);
+        KD_LAUNCH_CHECK("k_tiles");
+        b0 = b1;
+    }
+    k_static_out<<<1, 1024, 0, s>>>(H, ne, Fqe, Fte, eo, nradii, Fq, Ft, out);
+    KD_LAUNCH_CHECK("k_static_out");
+    int herr = 0;
+    check(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaMemcpyAsync(h_out, out, sizeof(long long) * (size_t)nradii * Fq * Ft,
+                          cudaMemcpyDeviceToHost, s), "D2H");
+    check(cudaStreamSynchronize(s), "sync");
+    if (herr) raise(herr, "node-pair traversal exceeded its stack");
+}
+
 }  // namespace kd
+
+extern "C" int kdg_count_static(const kd_catalog *tree, int Ft, const kd_catalog *query, int Fq,
+                                const double *rsq_sorted, int ne, const int *edge_of,
+                                int nradii, int mode, long long *out)
+{
+    if (ne < 0 || ne > KD_MAX_EDGES || nradii < 0 || nradii > KD_MAX_EDGES) {
+        kd_set_error(KD_EINVAL, "at most %d radii", KD_MAX_EDGES);
+        return KD_EINVAL;
+    }
+    try {
+        kd::count_static_impl(tree, Ft, query, Fq, rsq_sorted, ne, edge_of, nradii, mode, out);
+        return KD_OK;
+    } catch (const kd::Error &e) {
+        kd_set_error(e.code, "%s", e.msg);
+        return e.code;
+    }
+}
 
 extern "C" int kdg_set_device(int device)
 {

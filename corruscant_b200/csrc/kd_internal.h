@@ -128,6 +128,14 @@ int kdg_count(const kd_catalog *tree, const kd_catalog *query,
 int kdg_radec2cart(const double *ra, const double *dec, const double *dist,
                    double *xyz, int n);
 
+/* kdg_count without allocations: every buffer comes from a static device
+ * array (kd_count.cu).  rsq_sorted: ne distinct sorted squared edges;
+ * edge_of[k]: index in rsq_sorted of radius k, -1 for a NaN radius; out: host
+ * array of nradii * Fq * Ft cumulative counts in the reference layout. */
+int kdg_count_static(const kd_catalog *tree, int Ft, const kd_catalog *query, int Fq,
+                     const double *rsq_sorted, int ne, const int *edge_of, int nradii,
+                     int mode, long long *out);
+
 /* cudaSetDevice for the calling thread, with the library's error reporting */
 int kdg_set_device(int device);
 

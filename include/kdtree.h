@@ -135,6 +135,31 @@ int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii,
                          int nradii, int mode, int shard, int nshards,
                          long long *out, kd_count_stats *stats);
 
+/* kd_count_radii for callers that cannot allocate device memory while they
+ * count: a service whose device memory is owned by a fixed-budget pool, a
+ * host that forbids cudaMalloc because it synchronizes the whole device and
+ * would stall its other streams, or code that must not grow the process's
+ * footprint mid-run.  No counterpart in the reference (which has no device
+ * code).  Same inputs and output as kd_count_radii (trees from
+ * tree_construct, host radii, host out array of nradii * Fq * Ft counts),
+ * identical counts, no statistics.
+ *
+ * It allocates nothing, host or device, and creates no stream or event: its
+ * buffers come from one fixed 32 MiB array in device memory that every GPU
+ * holding the library keeps until the process exits; it runs on the legacy
+ * default stream and returns when the counts are on the host.  Limits: at
+ * most 64 radii; the bin histogram ((distinct radii + 1) x (max query field
+ * + 1) x (max tree field + 1) x 8 bytes) plus 16 bytes per query block of up
+ * to 128 points must leave room for tile records, and a single query block's
+ * tile records must fit (a clear error otherwise); larger jobs run in more
+ * batches, so this is slower than kd_count_radii.  The first call on a
+ * device looks up the array's device address (keep that first call outside
+ * any stream capture).  All calls share the array and its contents persist
+ * between calls; each call clears what it needs, but calls that overlap on
+ * the same GPU (other threads) race and must be serialised by the caller. */
+int kd_count_radii_static(kdtree_t tree, kdtree_t query, const double *radii,
+                          int nradii, int mode, long long *out);
+
 /* Same, with arbitrary query points (interleaved xyz, fields may be NULL). */
 int kd_count_points(kdtree_t tree, const double *xyz, const int *fields,
                     int length, int num_fields, const double *radii,
