@@ -245,59 +245,60 @@ __device__ __forceinline__ float fma_sat(float a, float b, float c)
 // in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals acc2 = sum c^2 bit
 // for bit when every c is 0 or 1; a band pair makes them differ by at least
 // 3/16, far above the FP32 rounding of these short sums (<= 256 terms <= 1).
+// Queries travel in pairs through the packed FP32 pipe (FFMA2/FADD2: two
+// independent round-to-nearest operations per instruction, the same values
+// as the scalar chain); the saturating ramp has no packed form and stays
+// scalar.  A staged point is (X, X, Y, Y), (Z, Z, N, N): each coordinate
+// twice, so one 16-byte shared load feeds both halves of a pair.
 // Returns a bit mask of the queries with a band pair.
 template <int K>
 __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int rl,
-                                             const float (&qx)[kQ], const float (&qy)[kQ],
-                                             const float (&qz)[kQ], const float (&a)[kQ][kPass32],
+                                             const float2 (&qx)[kQ / 2],
+                                             const float2 (&qy)[kQ / 2],
+                                             const float2 (&qz)[kQ / 2],
+                                             const float (&a)[kQ][kPass32],
                                              const float (&nsl)[kPass32], int (&cnt)[kQ][4])
 {
-    float acc[kQ][K], acc2[kQ];
+    float2 acc[kQ / 2][K], acc2[kQ / 2];
 #pragma unroll
-    for (int p = 0; p < kQ; p++) {
-        acc2[p] = 0.0f;
+    for (int h = 0; h < kQ / 2; h++) {
+        acc2[h] = make_float2(0.0f, 0.0f);
 #pragma unroll
-        for (int k = 0; k < K; k++) acc[p][k] = 0.0f;
+        for (int k = 0; k < K; k++) acc[h][k] = make_float2(0.0f, 0.0f);
     }
-    int j = 0;
-    for (; j + 2 <= rl; j += 2) {
-        const float4 t[2] = {ts[j], ts[j + 1]};
+    auto point = [&](const float4 xy, const float4 zn) {
+        const float2 X = make_float2(xy.x, xy.y), Y = make_float2(xy.z, xy.w);
+        const float2 Z = make_float2(zn.x, zn.y), N = make_float2(zn.z, zn.w);
 #pragma unroll
-        for (int u = 0; u < 2; u++)
-#pragma unroll
-            for (int p = 0; p < kQ; p++) {
-                const float s = fmaf(qz[p], t[u].z, fmaf(qy[p], t[u].y, fmaf(qx[p], t[u].x, t[u].w)));
-#pragma unroll
-                for (int k = 0; k < K; k++) {
-                    const float c = fma_sat(s, nsl[k], a[p][k]);
-                    acc[p][k] += c;
-                    acc2[p] = fmaf(c, c, acc2[p]);
-                }
-            }
-    }
-    if (j < rl) {
-        const float4 t = ts[j];
-#pragma unroll
-        for (int p = 0; p < kQ; p++) {
-            const float s = fmaf(qz[p], t.z, fmaf(qy[p], t.y, fmaf(qx[p], t.x, t.w)));
+        for (int h = 0; h < kQ / 2; h++) {
+            const float2 s = __ffma2_rn(qz[h], Z, __ffma2_rn(qy[h], Y, __ffma2_rn(qx[h], X, N)));
 #pragma unroll
             for (int k = 0; k < K; k++) {
-                const float c = fma_sat(s, nsl[k], a[p][k]);
-                acc[p][k] += c;
-                acc2[p] = fmaf(c, c, acc2[p]);
+                const float2 c = make_float2(fma_sat(s.x, nsl[k], a[2 * h][k]),
+                                             fma_sat(s.y, nsl[k], a[2 * h + 1][k]));
+                acc[h][k] = __fadd2_rn(acc[h][k], c);
+                acc2[h] = __ffma2_rn(c, c, acc2[h]);
             }
         }
+    };
+    int j = 0;
+    for (; j + 2 <= rl; j += 2) {
+        const float4 t0 = ts[2 * j], t1 = ts[2 * j + 1], t2 = ts[2 * j + 2], t3 = ts[2 * j + 3];
+        point(t0, t1);
+        point(t2, t3);
     }
+    if (j < rl) point(ts[2 * j], ts[2 * j + 1]);
     unsigned band = 0;
 #pragma unroll
     for (int p = 0; p < kQ; p++) {
         float tot = 0.0f;
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            tot += acc[p][k];
-            cnt[p][k] = __float2int_rn(acc[p][k]);
+            const float v = p & 1 ? acc[p >> 1][k].y : acc[p >> 1][k].x;
+            tot += v;
+            cnt[p][k] = __float2int_rn(v);
         }
-        if (tot != acc2[p]) band |= 1u << p;
+        if (tot != (p & 1 ? acc2[p >> 1].y : acc2[p >> 1].x)) band |= 1u << p;
     }
     return band;
 }
@@ -381,7 +382,7 @@ template <int MODE> struct WarpSmem {
     float Aw[KD_MAX_EDGES];
     float nsl[KD_MAX_EDGES];
     int uq[kMaxDistinctQf];
-    float4 stage[MODE == KD_MODE_MIXED ? KD_RUN_MAX : 1];
+    float4 stage[MODE == KD_MODE_MIXED ? 2 * KD_RUN_MAX : 1];  // (X,X,Y,Y), (Z,Z,N,N)
     double stage64[MODE == KD_MODE_FP64 ? 3 * KD_RUN_MAX : 1];
 };
 
@@ -393,9 +394,11 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *R = (double *)smem;  // ne
     WarpSmem<MODE> *ws = (WarpSmem<MODE> *)(R + KD_MAX_EDGES) + w;
-    // per-query bin counters: P[(e * kQ + p) * 32 + lane]
-    int *P = (int *)((WarpSmem<MODE> *)(R + KD_MAX_EDGES) + kTileWarpsPerCta) +
-             (size_t)w * (ne + 1) * kQ * 32;
+    // per-query bin counters, two queries per word, 16 bits each (a flush
+    // empties them before any could pass 65535): P[(e * kQ / 2 + h) * 32 + lane]
+    // holds queries 2h (low half) and 2h + 1 (high half)
+    unsigned *P = (unsigned *)((WarpSmem<MODE> *)(R + KD_MAX_EDGES) + kTileWarpsPerCta) +
+                  (size_t)w * (ne + 1) * (kQ / 2) * 32;
     for (int k = threadIdx.x; k < ne; k += blockDim.x) R[k] = A.rsq[k];
     __syncthreads();
     unsigned long long pairs = 0, rechecked = 0, wide = 0, kpairs = 0, wtiles = 0;
@@ -431,6 +434,18 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             qn[p] = (float)((double)qx[p] * qx[p] + (double)qy[p] * qy[p] + (double)qz[p] * qz[p]);
         }
         const int nvalid = __popc(vmask);
+        float2 qx2[kQ / 2], qy2[kQ / 2], qz2[kQ / 2];
+#pragma unroll
+        for (int h = 0; h < kQ / 2; h++) {
+            qx2[h] = make_float2(qx[2 * h], qx[2 * h + 1]);
+            qy2[h] = make_float2(qy[2 * h], qy[2 * h + 1]);
+            qz2[h] = make_float2(qz[2 * h], qz[2 * h + 1]);
+        }
+        // packed increment of the two queries of word h (invalid ones add 0)
+        auto pk = [&](int h, int d0, int d1) {
+            return (((vmask >> (2 * h)) & 1) ? (unsigned)d0 : 0u) |
+                   ((((vmask >> (2 * h + 1)) & 1) ? (unsigned)d1 : 0u) << 16);
+        };
         auto qfield = [&](int p) { return ((vmask >> p) & 1) ? A.Q.qf[qbase + p] : -1; };
         // the distinct own fields of the block (up to kMaxDistinctQf are
         // reduced per warp at a flush; beyond that, per-query atomics)
@@ -469,7 +484,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
         }
         for (int e = 0; e <= ne; e++)
 #pragma unroll
-            for (int p = 0; p < kQ; p++) P[(e * kQ + p) * 32 + lane] = 0;
+            for (int h = 0; h < kQ / 2; h++) P[(e * (kQ / 2) + h) * 32 + lane] = 0;
         __syncwarp();
         int cur_tf = -1;
         long long since = 0;
@@ -481,9 +496,11 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             for (int e = 0; e < ne; e++) {
                 int v[kQ];
 #pragma unroll
-                for (int p = 0; p < kQ; p++) {
-                    v[p] = P[(e * kQ + p) * 32 + lane];
-                    P[(e * kQ + p) * 32 + lane] = 0;
+                for (int h = 0; h < kQ / 2; h++) {
+                    const unsigned wv = P[(e * (kQ / 2) + h) * 32 + lane];
+                    P[(e * (kQ / 2) + h) * 32 + lane] = 0;
+                    v[2 * h] = (int)(wv & 0xFFFFu);
+                    v[2 * h + 1] = (int)(wv >> 16);
                 }
                 if (nuq <= kMaxDistinctQf) {
                     for (int u = 0; u < nuq; u++) {
@@ -505,7 +522,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                 }
             }
 #pragma unroll
-            for (int p = 0; p < kQ; p++) P[(ne * kQ + p) * 32 + lane] = 0;
+            for (int h = 0; h < kQ / 2; h++) P[(ne * (kQ / 2) + h) * 32 + lane] = 0;
         };
 
         // the next record's loads, held in registers while the current run
@@ -552,8 +569,10 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                             const float lx = fmaf(-0.5f, v2[h].x, dx);
                             const float ly = fmaf(-0.5f, v2[h].y, dy);
                             const float lz = fmaf(-0.5f, v2[h].z, dz);
-                            ws->stage[j] = make_float4(-2.0f * lx, -2.0f * ly, -2.0f * lz,
-                                                       fmaf(lz, lz, fmaf(ly, ly, lx * lx)));
+                            const float X = -2.0f * lx, Y = -2.0f * ly, Z = -2.0f * lz;
+                            const float N = fmaf(lz, lz, fmaf(ly, ly, lx * lx));
+                            ws->stage[2 * j] = make_float4(X, X, Y, Y);
+                            ws->stage[2 * j + 1] = make_float4(Z, Z, N, N);
                         }
                     }
                 } else {
@@ -572,7 +591,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             __syncwarp();
             if (i + 1 < ecnt) issue(i + 1);
 
-            if (tf != cur_tf || since > (1LL << 30)) {
+            if (tf != cur_tf || since + rl > 0xFFFF) {
                 if (cur_tf >= 0) flush(cur_tf);
                 cur_tf = tf;
                 since = 0;
@@ -580,8 +599,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             since += rl;
             if (K == 0) {
 #pragma unroll
-                for (int p = 0; p < kQ; p++)
-                    if ((vmask >> p) & 1) P[(k0 * kQ + p) * 32 + lane] += rl;
+                for (int h = 0; h < kQ / 2; h++) P[(k0 * (kQ / 2) + h) * 32 + lane] += pk(h, rl, rl);
                 __syncwarp();
                 continue;
             }
@@ -606,10 +624,10 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     }
                     unsigned band;
                     switch (kn) {
-                    case 1: band = fp32_run<1>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
-                    case 2: band = fp32_run<2>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
-                    case 3: band = fp32_run<3>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
-                    default: band = fp32_run<4>(ws->stage, rl, qx, qy, qz, a, sl, cnt); break;
+                    case 1: band = fp32_run<1>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
+                    case 2: band = fp32_run<2>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
+                    case 3: band = fp32_run<3>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
+                    default: band = fp32_run<4>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
                     }
                     redo = band & vmask;
                     rechecked += (unsigned long long)__popc(redo) * rl;
@@ -642,19 +660,19 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         for (int k = 0; k < 4; k++) cnt[p][k] = (pk >> (8 * k)) & 0xFF;
                     }
 #pragma unroll
-                for (int p = 0; p < kQ; p++)
-                    if ((vmask >> p) & 1) {
+                for (int h = 0; h < kQ / 2; h++)
 #pragma unroll
-                        for (int k = 0; k < 4; k++)
-                            if (k < kn) {
-                                P[((k0 + kb + k) * kQ + p) * 32 + lane] += cnt[p][k] - prev[p];
-                                prev[p] = cnt[p][k];
-                            }
-                    }
+                    for (int k = 0; k < 4; k++)
+                        if (k < kn) {
+                            P[((k0 + kb + k) * (kQ / 2) + h) * 32 + lane] +=
+                                pk(h, cnt[2 * h][k] - prev[2 * h], cnt[2 * h + 1][k] - prev[2 * h + 1]);
+                            prev[2 * h] = cnt[2 * h][k];
+                            prev[2 * h + 1] = cnt[2 * h + 1][k];
+                        }
             }
 #pragma unroll
-            for (int p = 0; p < kQ; p++)
-                if ((vmask >> p) & 1) P[((k0 + K) * kQ + p) * 32 + lane] += rl - prev[p];
+            for (int h = 0; h < kQ / 2; h++)
+                P[((k0 + K) * (kQ / 2) + h) * 32 + lane] += pk(h, rl - prev[2 * h], rl - prev[2 * h + 1]);
             const unsigned long long tp = (unsigned long long)nvalid * rl;
             pairs += tp;
             kpairs += tp * K;
@@ -684,7 +702,7 @@ static size_t tile_smem(int ne, int mode)
     const size_t ws = mode == KD_MODE_MIXED ? sizeof(WarpSmem<KD_MODE_MIXED>)
                                             : sizeof(WarpSmem<KD_MODE_FP64>);
     return sizeof(double) * KD_MAX_EDGES + ws * kTileWarpsPerCta +
-           sizeof(int) * (size_t)(ne + 1) * kQ * 32 * kTileWarpsPerCta;
+           sizeof(unsigned) * (size_t)(ne + 1) * (kQ / 2) * 32 * kTileWarpsPerCta;
 }
 
 struct Events {
