@@ -296,7 +296,9 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
         for (int k = 0; k < K; k++) {
             const float v = p & 1 ? acc[p >> 1][k].y : acc[p >> 1][k].x;
             tot += v;
-            cnt[p][k] = __float2int_rn(v);
+            // nearest integer of 0 <= v <= 256 without the conversion unit:
+            // v + 1.5 * 2^23 lands on the integer grid of that binade
+            cnt[p][k] = __float_as_int(v + 12582912.0f) - 0x4B400000;
         }
         if (tot != (p & 1 ? acc2[p >> 1].y : acc2[p >> 1].x)) band |= 1u << p;
     }
@@ -487,13 +489,15 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             for (int h = 0; h < kQ / 2; h++) P[(e * (kQ / 2) + h) * 32 + lane] = 0;
         __syncwarp();
         int cur_tf = -1;
-        long long since = 0;
+        int since = 0;
+        int tlo = ne, thi = -1;  // bins written since the last flush
 
         auto flush = [&](int tf) {
             int qf[kQ];
 #pragma unroll
             for (int p = 0; p < kQ; p++) qf[p] = qfield(p);
-            for (int e = 0; e < ne; e++) {
+            const int ehi = min(thi, ne - 1);
+            for (int e = tlo; e <= ehi; e++) {
                 int v[kQ];
 #pragma unroll
                 for (int h = 0; h < kQ / 2; h++) {
@@ -521,8 +525,12 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                                       (unsigned long long)v[p]);
                 }
             }
+            if (thi == ne) {
 #pragma unroll
-            for (int h = 0; h < kQ / 2; h++) P[(ne * (kQ / 2) + h) * 32 + lane] = 0;
+                for (int h = 0; h < kQ / 2; h++) P[(ne * (kQ / 2) + h) * 32 + lane] = 0;
+            }
+            tlo = ne;
+            thi = -1;
         };
 
         // the next record's loads, held in registers while the current run
@@ -597,6 +605,8 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                 since = 0;
             }
             since += rl;
+            tlo = min(tlo, k0);
+            thi = max(thi, k0 + K);
             if (K == 0) {
 #pragma unroll
                 for (int h = 0; h < kQ / 2; h++) P[(k0 * (kQ / 2) + h) * 32 + lane] += pk(h, rl, rl);
