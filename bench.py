@@ -10,15 +10,19 @@ Workload (the clustered 3-D autocorrelation the headline metric is quoted on):
   fields   64 jackknife fields on a 4x4x4 grid: 16*floor(4x)+4*floor(4y)+floor(4z)
 Synthetic inputs of the named shapes (no dataset is involved).
 
-A step is DD + DR + RR for all 21 edges (kd_count_radii on prebuilt trees,
-inputs resident in HBM).  value = pairs tested per second, all ranks, with
-the mixed FP32 + FP64-recheck counter; the plain FP64 counter is timed on the
-same steps.  e2e = the same pairs per second through the C ABI from host
-buffers: tree_construct of both catalogs (H2D of the points, node arrays back
-to the host), the three counts, results read back, every step.
+A step is DD + DR + RR for all 21 edges: one kd_count_batch call on prebuilt
+trees, inputs resident in HBM.  value = pairs tested per second, all ranks,
+with the mixed FP32 + FP64-recheck counter; the plain FP64 counter is timed
+on the same steps.  e2e = the same pairs per second through the C ABI from
+host buffers: tree_construct of both catalogs (H2D of the points, node arrays
+back to the host), the batched count, results read back, every step.  Also
+reported: the FP64 form against a measured DGEMM peak, the all-pairs-
+equivalent rate (Nd^2 + Nd Nr + Nr^2 per step over the step time) and an
+FP32-pipe model of the binning (FMA lane-ops per pair from the measured
+active edges per pair).
 
 --gpus N (torchrun): every rank builds the trees and counts its 1/N share of
-the query blocks (kd_count_radii_shard); the per-rank counts are summed with
+the batch's query blocks (kd_count_batch_shard); the per-rank counts are summed with
 one all-reduce and checked against rank 0's expectations.  Total work is
 fixed: scaling "strong".
 
@@ -124,16 +128,17 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def fp32_peak_tflops(device):
-    """Measured FP32 (CUDA-core) peak: cuBLAS SGEMM 8192^3 with TF32 off,
-    best of 5 (the FP32 analogue of the driver's bf16 GEMM measurement)."""
+def gemm_peak_tflops(device, dtype="float32"):
+    """Measured FP32 or FP64 peak: cuBLAS SGEMM (TF32 off) or DGEMM 8192^3,
+    best of 5 (the analogue of the driver's bf16 GEMM measurement)."""
     try:
         import torch
         torch.backends.cuda.matmul.allow_tf32 = False
         dev = torch.device("cuda", device)
         n = 8192
-        a = torch.randn(n, n, device=dev)
-        b = torch.randn(n, n, device=dev)
+        dt = getattr(torch, dtype)
+        a = torch.randn(n, n, device=dev, dtype=dt)
+        b = torch.randn(n, n, device=dev, dtype=dt)
         for _ in range(2):
             torch.mm(a, b)
         torch.cuda.synchronize(dev)
@@ -149,13 +154,21 @@ def fp32_peak_tflops(device):
         torch.cuda.empty_cache()
         return 2.0 * n ** 3 / best / 1e12
     except Exception as exc:  # no torch / no device: report without it
-        print(f"fp32 peak measurement unavailable: {exc}", file=sys.stderr)
+        print(f"{dtype} peak measurement unavailable: {exc}", file=sys.stderr)
+        return None
+
+
+def sm_count(device):
+    try:
+        import torch
+        return torch.cuda.get_device_properties(device).multi_processor_count
+    except Exception:
         return None
 
 
 def shard_range(n, shard, nshards):
     """[lo, hi) of shard `shard` of n items split evenly over nshards, the
-    split kd_count_radii_shard applies to query blocks."""
+    split kd_count_radii_shard and kd_count_batch_shard apply to query blocks."""
     return n * shard // nshards, n * (shard + 1) // nshards
 
 
@@ -206,42 +219,40 @@ def run_mine(args):
     td = N.build_tree(data, fd, N_FIELDS)
     tr = N.build_tree(rand, fr, N_FIELDS)
     build_s = time.perf_counter() - t0
-    jobs = (("DD", td, td), ("DR", tr, td), ("RR", tr, tr))
+    names = ("DD", "DR", "RR")
+    jobs = [(td, td), (tr, td), (tr, tr)]
 
     def step(mode):
-        out, stats = {}, {}
-        for name, t, q in jobs:
-            out[name], stats[name] = N.count_radii_shard(t, q, radii, D.rank, D.world, mode=mode,
-                                                         with_stats=True)
-        return out, stats
+        # DD, DR and RR in one device batch (kd_count_batch): one traversal
+        # and one persistent tile launch over all three counts' query blocks
+        outs, stats = N.count_batch(jobs, radii, mode=mode, with_stats=True, shard=D.rank,
+                                    nshards=D.world)
+        return dict(zip(names, outs)), stats
 
     def timed(mode, k, w):
         for _ in range(w):
             step(mode)
         D.barrier()
-        dev_ms, pairs, launches, res = 0.0, 0, 0, None
-        tiles_ms, tiles_pairs, rr_tiles_ms, rr_pairs = 0.0, 0, 0.0, 0
-        rechecked = 0
+        acc = dict(dev_ms=0.0, pairs=0, launches=0, tile_launches=0, tiles_ms=0.0, rechecked=0,
+                   edge_pairs=0)
+        res = None
         t0 = time.perf_counter()
         for _ in range(k):
-            res, st = step(mode)
-            for name, s in st.items():
-                dev_ms += s["ms_total"]
-                pairs += s["pairs_tested"]
-                launches += s["launches"]
-                rechecked += s["pairs_rechecked"]
-                tiles_ms += s["ms_tiles"]
-                tiles_pairs += s["pairs_tested"]
-                if name == "RR":
-                    rr_tiles_ms += s["ms_tiles"] / max(1, s["tile_launches"])
-                    rr_pairs += s["pairs_tested"] / max(1, s["tile_launches"])
-        wall = time.perf_counter() - t0
+            res, s = step(mode)
+            acc["dev_ms"] += s["ms_total"]
+            acc["pairs"] += s["pairs_tested"]
+            acc["launches"] += s["launches"]
+            acc["tile_launches"] += s["tile_launches"]
+            acc["tiles_ms"] += s["ms_tiles"]
+            acc["rechecked"] += s["pairs_rechecked"]
+            acc["edge_pairs"] += s["edge_pairs"]
+        acc["wall"] = time.perf_counter() - t0
+        acc["res"] = res
         D.barrier()
-        return dict(dev_ms=dev_ms, pairs=pairs, launches=launches, wall=wall, res=res,
-                    tiles_ms=tiles_ms, tiles_pairs=tiles_pairs, rechecked=rechecked,
-                    rr_launch_ms=rr_tiles_ms / k, rr_launch_pairs=rr_pairs / k)
+        return acc
 
-    peak = fp32_peak_tflops(D.local) if D.rank == 0 else None
+    peak = gemm_peak_tflops(D.local, "float32") if D.rank == 0 else None
+    peak64 = gemm_peak_tflops(D.local, "float64") if D.rank == 0 else None
     with ClockSampler(D.local) as clk:
         mixed = timed(N.KD_MODE_MIXED, args.steps, args.warmup)
     clocks = clk.summary()
@@ -263,10 +274,9 @@ def run_mine(args):
         t0 = time.perf_counter()
         a = N.build_tree(data, fd, N_FIELDS)
         b = N.build_tree(rand, fr, N_FIELDS)
-        p = 0
-        for name, t, q in (("DD", a, a), ("DR", b, a), ("RR", b, b)):
-            _, s = N.count_radii_shard(t, q, radii, D.rank, D.world, with_stats=True)
-            p += s["pairs_tested"]
+        _, s = N.count_batch([(a, a), (b, a), (b, b)], radii, with_stats=True, shard=D.rank,
+                             nshards=D.world)
+        p = s["pairs_tested"]
         dt = time.perf_counter() - t0
         d2h = 40 * (a.memsize + b.memsize) + 3 * 8 * len(radii) * N_FIELDS * N_FIELDS
         N.destroy(a)
@@ -285,15 +295,38 @@ def run_mine(args):
 
     if D.rank == 0:
         value = pairs / dev_s
-        achieved = mixed["rr_launch_pairs"] * FLOP_PER_PAIR / (mixed["rr_launch_ms"] * 1e-3) / 1e12
+        # the dominant kernel: k_tiles, one launch per step (DD+DR+RR batch)
+        launch_pairs = mixed["pairs"] / max(1, mixed["tile_launches"])
+        launch_ms = mixed["tiles_ms"] / max(1, mixed["tile_launches"])
+        achieved = launch_pairs * FLOP_PER_PAIR / (launch_ms * 1e-3) / 1e12
         roofline = {"bound": "fp32", "achieved": achieved,
                     "peak": peak, "unit": "TFLOP/s",
                     "frac": (achieved / peak) if peak else None,
-                    "traffic": TILE_TRAFFIC_PER_PAIR * mixed["rr_launch_pairs"]
+                    "traffic": TILE_TRAFFIC_PER_PAIR * launch_pairs
                     if TILE_TRAFFIC_PER_PAIR else None,
-                    "kernel": "k_tiles<mixed> (RR launch)",
+                    "kernel": "k_tiles<mixed> (one launch: DD+DR+RR batch)",
                     "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off",
                     "flop_per_pair": FLOP_PER_PAIR}
+        # FP32-pipe model of the binning itself: per pair 3 FMA lane-ops for
+        # the distance and 3 per active edge (ramp, count, band check)
+        kbar = mixed["edge_pairs"] / max(1, mixed["pairs"])
+        nsm, mhz = sm_count(D.local), clocks.get("sm_mhz")
+        ops = 3.0 + 3.0 * kbar
+        pipe_bound = 128.0 * nsm * mhz * 1e6 / ops if (nsm and mhz) else None
+        tile_rate = launch_pairs / (launch_ms * 1e-3)
+        pipe_model = {"active_edges_per_pair": kbar, "fma_lane_ops_per_pair": ops,
+                      "bound_pairs_per_s": pipe_bound,
+                      "frac": tile_rate / pipe_bound if pipe_bound else None,
+                      "basis": "128 FP32 lanes/SM/clock x SMs x median SM clock"}
+        f_launch_pairs = fp64["pairs"] / max(1, fp64["tile_launches"])
+        f_launch_ms = fp64["tiles_ms"] / max(1, fp64["tile_launches"])
+        f_achieved = f_launch_pairs * FLOP_PER_PAIR / (f_launch_ms * 1e-3) / 1e12
+        fp64_roofline = {"bound": "fp64", "achieved": f_achieved, "peak": peak64,
+                         "unit": "TFLOP/s", "frac": (f_achieved / peak64) if peak64 else None,
+                         "kernel": "k_tiles<fp64>",
+                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"}
+        nd, nr = len(data), len(rand)
+        all_pairs = float(nd) * nd + float(nr) * nd + float(nr) * nr
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world,
             "steps": args.steps, "warmup": args.warmup,
@@ -305,7 +338,9 @@ def run_mine(args):
                        "parallelism": f"query blocks sharded over {D.world} GPU(s)",
                        "l2": "inputs larger than L2 (20M tree points: 640 MB FP64 + 320 MB FP32)"},
             "fp64_form": {"value": fpairs / fdev_s, "ms_per_step": fdev_s / args.steps * 1e3,
-                          "dtype": "f64"},
+                          "dtype": "f64", "roofline": fp64_roofline},
+            "all_pairs_equivalent_per_s": all_pairs / (dev_s / args.steps),
+            "fp32_pipe_model": pipe_model,
             "mixed_over_fp64": (pairs / dev_s) / (fpairs / fdev_s),
             "counts_exact_mixed_vs_fp64": bool(exact),
             "recheck_rate": rechecked / max(1, pairs),

@@ -93,6 +93,13 @@ def kdlib():
         L.kd_count_radii_shard.restype = c_int
         L.kd_count_radii_shard.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int, c_int,
                                            c_int, POINTER(c_longlong), POINTER(CountStats)]
+        L.kd_count_batch_shard.restype = c_int
+        L.kd_count_batch_shard.argtypes = [POINTER(KdTree), POINTER(KdTree), c_int, POINTER(c_double),
+                                           c_int, c_int, c_int, c_int, POINTER(c_longlong),
+                                           POINTER(CountStats)]
+        L.kd_count_batch.restype = c_int
+        L.kd_count_batch.argtypes = [POINTER(KdTree), POINTER(KdTree), c_int, POINTER(c_double),
+                                     c_int, c_int, POINTER(c_longlong), POINTER(CountStats)]
         L.kd_count_radii_static.restype = c_int
         L.kd_count_radii_static.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int,
                                             POINTER(c_longlong)]
@@ -175,6 +182,28 @@ def count_radii_shard(tree, query, radii, shard, nshards, mode=KD_MODE_MIXED, wi
     if rc != 0:
         raise_last()
     return (out, st.as_dict()) if with_stats else out
+
+
+def count_batch(jobs, radii, mode=KD_MODE_MIXED, with_stats=False, shard=0, nshards=1):
+    """kd_count_batch: jobs is a sequence of (tree, query tree) pairs; returns
+    one count_radii result per job (all jobs counted in one device batch)."""
+    jobs = list(jobs)
+    radii = np.require(np.asarray(radii, dtype=np.float64), requirements="AC")
+    trees = (KdTree * len(jobs))(*[t for t, _ in jobs])
+    queries = (KdTree * len(jobs))(*[q for _, q in jobs])
+    sizes = [len(radii) * q.num_fields * t.num_fields for t, q in jobs]
+    flat = np.zeros(max(1, sum(sizes)), dtype=np.int64)
+    st = CountStats()
+    rc = kdlib().kd_count_batch_shard(trees, queries, c_int(len(jobs)), dptr(radii),
+                                      c_int(len(radii)), c_int(mode), c_int(shard), c_int(nshards),
+                                      flat.ctypes.data_as(POINTER(c_longlong)), ctypes.byref(st))
+    if rc != 0:
+        raise_last()
+    outs, at = [], 0
+    for (t, q), n in zip(jobs, sizes):
+        outs.append(flat[at:at + n].reshape(len(radii), q.num_fields * t.num_fields).copy())
+        at += n
+    return (outs, st.as_dict()) if with_stats else outs
 
 
 def count_radii_static(tree, query, radii, mode=KD_MODE_MIXED):

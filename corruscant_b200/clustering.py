@@ -7,9 +7,10 @@ User API of the reference module ``corruscant.clustering``
 and error behaviour.
 
 What changes is below the API: a ``tree`` is built on the GPU (bit-identical
-node array), and ``_autocorr`` / ``_crosscorr`` count every bin edge in one
-GPU pass per count type (``kd_count_radii``) instead of one ``pair_count``
-call per edge (clustering.py:218-230, :256-284).  The per-edge cumulative
+node array), and ``_autocorr`` / ``_crosscorr`` count every bin edge of every
+count type (DD, DR, RR, or the four cross counts) in one GPU batch
+(``kd_count_batch``) instead of one ``pair_count`` call per edge and count
+type (clustering.py:218-230, :256-284).  The per-edge cumulative
 counts, their ``np.diff`` and everything downstream are the same numbers.
 
 The estimator, error and covariance arithmetic is performed in the same
@@ -158,8 +159,15 @@ def _query_tree(tree_, points, radius, num_threads, fields=None, N_fields=1):
 def _count_binned(tree_, query, radii, mode):
     """Per-bin (len(radii)-1, Fq, Ft) counts of ``query``'s points against
     ``tree_``: the np.diff over edges of the per-edge cumulative counts."""
-    cum = _native.count_radii(tree_.ctree, query.ctree, radii, mode=mode)
-    return np.diff(cum.reshape(len(radii), query.N_fields, tree_.N_fields), axis=0)
+    return _count_binned_batch([(tree_, query)], radii, mode)[0]
+
+
+def _count_binned_batch(jobs, radii, mode):
+    """_count_binned for several (tree, query) pairs, counted together in one
+    device batch (``kd_count_batch``)."""
+    cums = _native.count_batch([(t.ctree, q.ctree) for t, q in jobs], radii, mode=mode)
+    return [np.diff(c.reshape(len(radii), q.N_fields, t.N_fields), axis=0)
+            for (t, q), c in zip(jobs, cums)]
 
 
 def _autocorr(data_tree, rand_tree, radii, est_type="landy-szalay", err_type="jackknife",
@@ -172,9 +180,8 @@ def _autocorr(data_tree, rand_tree, radii, est_type="landy-szalay", err_type="ja
     estimator = _estimator(est_type)
     mode = DEFAULT_MODE if mode is None else mode
     radii = np.asarray(radii, dtype="float64")
-    dd = _count_binned(data_tree, data_tree, radii, mode)
-    dr = _count_binned(rand_tree, data_tree, radii, mode)
-    rr = _count_binned(rand_tree, rand_tree, radii, mode)
+    dd, dr, rr = _count_binned_batch(
+        [(data_tree, data_tree), (rand_tree, data_tree), (rand_tree, rand_tree)], radii, mode)
     return autocorr_results(dd, dr, rr, data_tree, rand_tree, estimator, radii)
 
 
@@ -191,15 +198,15 @@ def _crosscorr(data_tree_1, data_tree_2, rand_tree_1, rand_tree_2, radii,
     mode = DEFAULT_MODE if mode is None else mode
     radii = np.asarray(radii, dtype="float64")
     if data_tree_1.size > data_tree_2.size:
-        d1d2 = _count_binned(data_tree_1, data_tree_2, radii, mode)
+        dd_job = (data_tree_1, data_tree_2)
     else:
-        d1d2 = _count_binned(data_tree_2, data_tree_1, radii, mode)
-    d1r2 = _count_binned(rand_tree_2, data_tree_1, radii, mode)
-    d2r1 = _count_binned(rand_tree_1, data_tree_2, radii, mode)
+        dd_job = (data_tree_2, data_tree_1)
     if rand_tree_1.size > rand_tree_2.size:
-        r1r2 = _count_binned(rand_tree_1, rand_tree_2, radii, mode)
+        rr_job = (rand_tree_1, rand_tree_2)
     else:
-        r1r2 = _count_binned(rand_tree_2, rand_tree_1, radii, mode)
+        rr_job = (rand_tree_2, rand_tree_1)
+    d1d2, d1r2, d2r1, r1r2 = _count_binned_batch(
+        [dd_job, (rand_tree_2, data_tree_1), (rand_tree_1, data_tree_2), rr_job], radii, mode)
     return crosscorr_results(d1d2, d1r2, d2r1, r1r2, data_tree_1, data_tree_2, rand_tree_1,
                              rand_tree_2, estimator, radii)
 

@@ -169,51 +169,56 @@ static int cmp_double(const void *a, const void *b)
 }
 
 /*
- * Count with the tree catalog and a query catalog for all radii and write the
- * reference's cumulative per-radius matrices, out[k][qf*Fq + tf]
- * (kdquery.c:34: rows strided by the QUERY field count Fq).
+ * Count njobs (tree catalog, query catalog) pairs for all radii in one device
+ * batch and write, job after job, the reference's cumulative per-radius
+ * matrices out[k][qf*Fq + tf] (kdquery.c:34: rows strided by the QUERY field
+ * count Fq), nradii * Fq[j] * Ft[j] values per job.
  */
-static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, int Fq,
-                          const double *radii, int nradii, int mode, int shard, int nshards,
-                          long long *out, kd_count_stats *stats)
+static int count_jobs(const kd_catalog *const *tcs, const int *Fts, const kd_catalog *const *qcs,
+                      const int *Fqs, int njobs, const double *radii, int nradii, int mode,
+                      int shard, int nshards, long long *out, kd_count_stats *stats)
 {
     double *rsq = NULL, *uniq = NULL;
-    long long *hist = NULL;
-    int k, ne = 0, rc = KD_OK;
-    size_t nrow = (size_t)Fq * (size_t)Ft;
+    long long **hists = NULL;
+    int j, k, ne = 0, rc = KD_OK;
+    size_t total = 0;
 
     if (mode != KD_MODE_MIXED && mode != KD_MODE_FP64) {
         kd_set_error(KD_EINVAL, "unknown count mode %d", mode);
         return KD_EINVAL;
     }
-    if (Fq < 1 || Ft < 1) {
-        kd_set_error(KD_EFIELD, "field counts must be positive");
-        return KD_EFIELD;
-    }
-    if (qc->min_qf < 0) {
-        kd_set_error(KD_EFIELD, "negative query field id");
-        return KD_EFIELD;
-    }
-    /* the reference would write outside its Fq*Ft counter (kdquery.c:34) */
-    if ((long long)qc->max_qf * Fq + tc->max_tf >= (long long)nrow) {
-        kd_set_error(KD_EFIELD, "field ids overflow the %d x %d counter (qfield*%d + tfield)",
-                     Fq, Ft, Fq);
-        return KD_EFIELD;
+    for (j = 0; j < njobs; j++) {
+        const int Fq = Fqs[j], Ft = Fts[j];
+        if (Fq < 1 || Ft < 1) {
+            kd_set_error(KD_EFIELD, "field counts must be positive");
+            return KD_EFIELD;
+        }
+        if (qcs[j]->min_qf < 0) {
+            kd_set_error(KD_EFIELD, "negative query field id");
+            return KD_EFIELD;
+        }
+        /* the reference would write outside its Fq*Ft counter (kdquery.c:34) */
+        if ((long long)qcs[j]->max_qf * Fq + tcs[j]->max_tf >= (long long)Fq * Ft) {
+            kd_set_error(KD_EFIELD, "field ids overflow the %d x %d counter (qfield*%d + tfield)",
+                         Fq, Ft, Fq);
+            return KD_EFIELD;
+        }
+        total += (size_t)Fq * (size_t)Ft * (size_t)nradii;
     }
     for (k = 0; k < nradii; k++)
         if (radii[k] < 0) {
             kd_set_error(KD_ERADIUS, "negative radius %g", radii[k]);
             return KD_ERADIUS;
         }
-    memset(out, 0, sizeof(long long) * nrow * (size_t)nradii);
+    memset(out, 0, sizeof(long long) * total);
     if (stats) memset(stats, 0, sizeof *stats);
     rsq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
     uniq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
-    if (!rsq || !uniq) {
-        free(rsq);
-        free(uniq);
+    hists = (long long **)calloc((size_t)njobs, sizeof(long long *));
+    if (!rsq || !uniq || !hists) {
         kd_set_error(KD_ENOMEM, "out of host memory");
-        return KD_ENOMEM;
+        rc = KD_ENOMEM;
+        goto done;
     }
     /* squared radii exactly as kdquery.c:77 forms them; NaN counts nothing */
     for (k = 0; k < nradii; k++) rsq[k] = radii[k] * radii[k];
@@ -231,21 +236,26 @@ static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, in
         rc = KD_EINVAL;
         goto done;
     }
-    if (ne > 0) {
-        const size_t Fqe = (size_t)qc->max_qf + 1, Fte = (size_t)tc->max_tf + 1;
-        const size_t hrow = Fqe * Fte;
-        hist = (long long *)calloc((size_t)(ne + 1) * hrow, sizeof(long long));
-        if (!hist) {
+    if (ne == 0) goto done;
+    for (j = 0; j < njobs; j++) {
+        const size_t hrow = ((size_t)qcs[j]->max_qf + 1) * ((size_t)tcs[j]->max_tf + 1);
+        hists[j] = (long long *)calloc((size_t)(ne + 1) * hrow, sizeof(long long));
+        if (!hists[j]) {
             kd_set_error(KD_ENOMEM, "out of host memory");
             rc = KD_ENOMEM;
             goto done;
         }
-        rc = kdg_count(tc, qc, uniq, ne, mode, shard, nshards, hist, stats);
-        if (rc != KD_OK) goto done;
+    }
+    rc = kdg_count_batch(tcs, qcs, njobs, uniq, ne, mode, shard, nshards, hists, stats);
+    if (rc != KD_OK) goto done;
+    for (j = 0; j < njobs; j++) {
+        const size_t Fqe = (size_t)qcs[j]->max_qf + 1, Fte = (size_t)tcs[j]->max_tf + 1;
+        const size_t hrow = Fqe * Fte, nrow = (size_t)Fqs[j] * (size_t)Fts[j];
+        long long *hist = hists[j];
         /* cumulative over sorted edges: pairs with d2 < uniq[e] */
         for (k = 1; k < ne; k++) {
-            size_t j;
-            for (j = 0; j < hrow; j++) hist[(size_t)k * hrow + j] += hist[(size_t)(k - 1) * hrow + j];
+            size_t i;
+            for (i = 0; i < hrow; i++) hist[(size_t)k * hrow + i] += hist[(size_t)(k - 1) * hrow + i];
         }
         for (k = 0; k < nradii; k++) {
             int lo = 0, hi = ne;
@@ -259,14 +269,24 @@ static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, in
             }
             for (qf = 0; qf < Fqe; qf++)
                 for (tf = 0; tf < Fte; tf++)
-                    o[qf * (size_t)Fq + tf] += hist[(size_t)lo * hrow + qf * Fte + tf];
+                    o[qf * (size_t)Fqs[j] + tf] += hist[(size_t)lo * hrow + qf * Fte + tf];
         }
+        out += nrow * (size_t)nradii;
     }
 done:
+    if (hists)
+        for (j = 0; j < njobs; j++) free(hists[j]);
+    free(hists);
     free(rsq);
     free(uniq);
-    free(hist);
     return rc;
+}
+
+static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, int Fq,
+                          const double *radii, int nradii, int mode, int shard, int nshards,
+                          long long *out, kd_count_stats *stats)
+{
+    return count_jobs(&tc, &Ft, &qc, &Fq, 1, radii, nradii, mode, shard, nshards, out, stats);
 }
 
 /* query catalog from raw points; NaN rows are dropped (they count nothing in
@@ -369,6 +389,58 @@ int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradi
                    long long *out, kd_count_stats *stats)
 {
     return kd_count_radii_shard(tree, query, radii, nradii, mode, 0, 1, out, stats);
+}
+
+int kd_count_batch_shard(const kdtree_t *trees, const kdtree_t *queries, int njobs,
+                         const double *radii, int nradii, int mode, int shard, int nshards,
+                         long long *out, kd_count_stats *stats)
+{
+    const kd_catalog **tcs = NULL, **qcs = NULL;
+    int *Fts = NULL, *Fqs = NULL;
+    int j, rc = KD_OK;
+    clear_error();
+    if (njobs < 1 || !trees || !queries || nradii < 0 || (nradii > 0 && !radii) || !out) {
+        kd_set_error(KD_EINVAL, "kd_count_batch: bad arguments");
+        return KD_EINVAL;
+    }
+    if (nshards < 1 || shard < 0 || shard >= nshards) {
+        kd_set_error(KD_EINVAL, "kd_count_batch: shard %d of %d", shard, nshards);
+        return KD_EINVAL;
+    }
+    tcs = (const kd_catalog **)malloc(sizeof(*tcs) * (size_t)njobs);
+    qcs = (const kd_catalog **)malloc(sizeof(*qcs) * (size_t)njobs);
+    Fts = (int *)malloc(sizeof(int) * (size_t)njobs);
+    Fqs = (int *)malloc(sizeof(int) * (size_t)njobs);
+    if (!tcs || !qcs || !Fts || !Fqs) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        rc = KD_ENOMEM;
+        goto done;
+    }
+    for (j = 0; j < njobs; j++) {
+        kd_handle *ht = lookup_or_fail(&trees[j], "kd_count_batch (tree)");
+        kd_handle *hq = ht ? lookup_or_fail(&queries[j], "kd_count_batch (query)") : NULL;
+        if (!ht || !hq) {
+            rc = KD_EINVAL;
+            goto done;
+        }
+        tcs[j] = &ht->cat;
+        qcs[j] = &hq->cat;
+        Fts[j] = trees[j].num_fields;
+        Fqs[j] = queries[j].num_fields;
+    }
+    rc = count_jobs(tcs, Fts, qcs, Fqs, njobs, radii, nradii, mode, shard, nshards, out, stats);
+done:
+    free(tcs);
+    free(qcs);
+    free(Fts);
+    free(Fqs);
+    return rc;
+}
+
+int kd_count_batch(const kdtree_t *trees, const kdtree_t *queries, int njobs, const double *radii,
+                   int nradii, int mode, long long *out, kd_count_stats *stats)
+{
+    return kd_count_batch_shard(trees, queries, njobs, radii, nradii, mode, 0, 1, out, stats);
 }
 
 int kd_count_radii_static(kdtree_t tree, kdtree_t query, const double *radii, int nradii,

@@ -32,6 +32,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
+#include <cstring>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -61,6 +63,33 @@ struct QuerySide {
     const int *blk_start, *blk_len, *blk_qf;
     const double *blk_box;
 };
+
+// One (tree, query tree) count of a batch.  A batch numbers the query blocks
+// of all its jobs consecutively: job j owns global blocks [jblk[j], jblk[j+1]).
+struct JobDesc {
+    TreeSide T;
+    QuerySide Q;
+    const double *tx, *ty, *tz;  // tree points, FP64, counting order
+    const float4 *t4;            // tree points: (-2 t_r, |t_r|^2), t_r relative to leaf centre
+    const double *leaf_c;        // 3 per leaf
+    double hT;                   // largest leaf half-diagonal, with margin
+    unsigned long long *H;       // (ne + 1) x Fqe x Fte bin histogram
+    int Fqe, Fte;
+};
+static_assert(sizeof(JobDesc) % 8 == 0, "JobDesc is copied in 8-byte words");
+
+// the job owning global block g: the last j with jblk[j] <= g (an empty job
+// shares its start with the next one, which is then the one found)
+__device__ __forceinline__ int job_of(const int *__restrict__ jblk, int njobs, int g)
+{
+    int lo = 0, hi = njobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (jblk[mid] <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
 
 // Bins a pair of boxes can reach: pairs land in bins elo..ehi (ne = beyond
 // every edge).  The box bounds are exact for the points' true distances; the
@@ -99,18 +128,19 @@ __device__ __forceinline__ void bin_range(const double *a, const double *b,
 // first active edge << 16 | active edge count << 24.
 struct TravOut {
     int *count;              // COUNT pass: tiles per block
-    const long long *off;    // FILL pass: batch-relative tile offsets
+    const long long *off;    // FILL pass: launch-relative tile offsets
     uint4 *rec;              // FILL: tile records
-    unsigned long long *H;
-    int Fqe, Fte;
     unsigned long long *accepted;
     int *err;
 };
 
+// one warp per global query block g in [g0, g1)
 template <bool FILL>
-__global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QuerySide Q,
+__global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__restrict__ jobs,
+                                                             const int *__restrict__ jblk,
+                                                             int njobs,
                                                              const double *__restrict__ g_rsq,
-                                                             int ne, int b0, int b1, TravOut o)
+                                                             int ne, int g0, int g1, TravOut o)
 {
     __shared__ int stack[kTravWarps][kStack];
     __shared__ double rsq[KD_MAX_EDGES];
@@ -118,8 +148,14 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
     for (int k = threadIdx.x; k < ne; k += blockDim.x) rsq[k] = g_rsq[k];
     __syncthreads();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int b = b0 + blockIdx.x * kTravWarps + w;
-    if (b >= b1) return;
+    const int g = g0 + blockIdx.x * kTravWarps + w;
+    if (g >= g1) return;
+    const int j = job_of(jblk, njobs, g);
+    const int b = g - jblk[j];
+    const TreeSide T = jobs[j].T;
+    const QuerySide Q = jobs[j].Q;
+    unsigned long long *const H = jobs[j].H;
+    const int Fqe = jobs[j].Fqe, Fte = jobs[j].Fte;
     const int alen = Q.blk_len[b], aqf = Q.blk_qf[b];
     double *bb = wb[w];
     if (lane < 6) bb[lane] = Q.blk_box[6 * (size_t)b + lane];
@@ -128,7 +164,7 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
     __syncwarp();
     int sp = 1;
     long long emitted = 0;
-    const long long base = FILL ? o.off[b - b0] : 0;
+    const long long base = FILL ? o.off[g - g0] : 0;
     unsigned long long acc_pairs = 0;
     long long guard = 4LL * T.nleaves + 64;
     while (sp > 0) {
@@ -149,7 +185,7 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
                 if (FILL) {
                     const unsigned long long c =
                         (unsigned long long)alen * (unsigned long long)T.count[h];
-                    atomicAdd(&o.H[((size_t)elo * o.Fqe + aqf) * o.Fte + T.tf[h]], c);
+                    atomicAdd(&H[((size_t)elo * Fqe + aqf) * Fte + T.tf[h]], c);
                     acc_pairs += c;
                 }
             } else if (h >= T.nleaves) {
@@ -196,7 +232,7 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(TreeSide T, QueryS
         emitted += etot;
         __syncwarp();
     }
-    if (!FILL && lane == 0) o.count[b - b0] = (int)emitted;
+    if (!FILL && lane == 0) o.count[g - g0] = (int)emitted;
     if (FILL) {
         for (int off = 16; off; off >>= 1) acc_pairs += __shfl_xor_sync(0xffffffffu, acc_pairs, off);
         if (lane == 0 && acc_pairs) atomicAdd(o.accepted, acc_pairs);
@@ -363,24 +399,21 @@ __device__ __noinline__ unsigned exact_pass(const double *__restrict__ tx,
 }
 
 struct TileArgs {
-    const double *tx, *ty, *tz;  // tree points, FP64, counting order
-    const float4 *t4;            // tree points: (-2 t_r, |t_r|^2), t_r relative to leaf centre
-    const double *leaf_c;        // 3 per leaf
-    double hT;                   // largest leaf half-diagonal
-    QuerySide Q;
+    const JobDesc *jobs;
+    const int *jblk;
+    int njobs;
     const double *rsq;
     int ne;
-    int b0, b1;
-    const long long *off;
+    int g0, g1;                 // global query blocks of this launch
+    const long long *off;       // launch-relative tile offsets
     const uint4 *rec;
-    unsigned long long *H;
-    int Fqe, Fte;
     int *work;
     unsigned long long *stats;  // tested, rechecked, accepted, wide, edge-pairs, warp tiles
 };
 
 // shared memory of one warp
 template <int MODE> struct WarpSmem {
+    JobDesc job;  // the job of the block being counted
     float Aw[KD_MAX_EDGES];
     float nsl[KD_MAX_EDGES];
     int uq[kMaxDistinctQf];
@@ -409,12 +442,21 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
         int item = 0;
         if (lane == 0) item = atomicAdd(A.work, 1);
         item = __shfl_sync(0xffffffffu, item, 0);
-        const int b = A.b0 + item;
-        if (b >= A.b1) break;
-        const int qlen = A.Q.blk_len[b], qs = A.Q.blk_start[b];
-        const long long eoff = A.off[b - A.b0];
-        const int ecnt = (int)(A.off[b - A.b0 + 1] - eoff);
-        const double *bx = A.Q.blk_box + 6 * (size_t)b;
+        const int g = A.g0 + item;
+        if (g >= A.g1) break;
+        const int jb = job_of(A.jblk, A.njobs, g);
+        {
+            const unsigned long long *src = (const unsigned long long *)(A.jobs + jb);
+            unsigned long long *dst = (unsigned long long *)&ws->job;
+            for (int u = lane; u < (int)(sizeof(JobDesc) / 8); u += 32) dst[u] = src[u];
+            __syncwarp();
+        }
+        const JobDesc &J = ws->job;
+        const int b = g - A.jblk[jb];
+        const int qlen = J.Q.blk_len[b], qs = J.Q.blk_start[b];
+        const long long eoff = A.off[g - A.g0];
+        const int ecnt = (int)(A.off[g - A.g0 + 1] - eoff);
+        const double *bx = J.Q.blk_box + 6 * (size_t)b;
         const double ox = 0.5 * (bx[0] + bx[3]), oy = 0.5 * (bx[1] + bx[4]),
                      oz = 0.5 * (bx[2] + bx[5]);
         // queries 4*lane .. 4*lane+3 of the block; their FP64 coordinates and
@@ -428,8 +470,8 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             const int j = kQ * lane + p;
             const bool v = j < qlen;
             vmask |= (unsigned)v << p;
-            const double xd = v ? A.Q.x[qs + j] : ox, yd = v ? A.Q.y[qs + j] : oy,
-                         zd = v ? A.Q.z[qs + j] : oz;
+            const double xd = v ? J.Q.x[qs + j] : ox, yd = v ? J.Q.y[qs + j] : oy,
+                         zd = v ? J.Q.z[qs + j] : oz;
             qx[p] = (float)(xd - ox);
             qy[p] = (float)(yd - oy);
             qz[p] = (float)(zd - oz);
@@ -448,7 +490,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             return (((vmask >> (2 * h)) & 1) ? (unsigned)d0 : 0u) |
                    ((((vmask >> (2 * h + 1)) & 1) ? (unsigned)d1 : 0u) << 16);
         };
-        auto qfield = [&](int p) { return ((vmask >> p) & 1) ? A.Q.qf[qbase + p] : -1; };
+        auto qfield = [&](int p) { return ((vmask >> p) & 1) ? J.Q.qf[qbase + p] : -1; };
         // the distinct own fields of the block (up to kMaxDistinctQf are
         // reduced per warp at a flush; beyond that, per-query atomics)
         int nuq = 0;
@@ -475,7 +517,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             const double Rq = sqrt(hx * hx + hy * hy + hz * hz) * (1.0 + 1e-12);
             for (int k = lane; k < ne; k += 32) {
                 if (isfinite(R[k])) {
-                    const double inv4e = 0.25 / band_halfwidth(R[k], Rq, A.hT);
+                    const double inv4e = 0.25 / band_halfwidth(R[k], Rq, J.hT);
                     ws->nsl[k] = (float)(-inv4e);
                     ws->Aw[k] = (float)(0.5 + R[k] * inv4e);
                 } else {
@@ -514,14 +556,14 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         for (int p = 0; p < kQ; p++) sum += qf[p] == uf ? v[p] : 0;
                         for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
                         if (lane == 0 && sum)
-                            atomicAdd(&A.H[((size_t)e * A.Fqe + uf) * A.Fte + tf],
+                            atomicAdd(&J.H[((size_t)e * J.Fqe + uf) * J.Fte + tf],
                                       (unsigned long long)sum);
                     }
                 } else {
 #pragma unroll
                     for (int p = 0; p < kQ; p++)
                         if (((vmask >> p) & 1) && v[p])
-                            atomicAdd(&A.H[((size_t)e * A.Fqe + qf[p]) * A.Fte + tf],
+                            atomicAdd(&J.H[((size_t)e * J.Fqe + qf[p]) * J.Fte + tf],
                                       (unsigned long long)v[p]);
                 }
             }
@@ -544,17 +586,17 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             if (K == 0) return;
             if (MODE == KD_MODE_MIXED) {
                 const unsigned rs = nrec.x, leaf = nrec.y;
-                ncx = A.leaf_c[3 * (size_t)leaf];
-                ncy = A.leaf_c[3 * (size_t)leaf + 1];
-                ncz = A.leaf_c[3 * (size_t)leaf + 2];
-                if (lane < rl) na = A.t4[rs + lane];
-                if (lane + 32 < rl) nb = A.t4[rs + lane + 32];
+                ncx = J.leaf_c[3 * (size_t)leaf];
+                ncy = J.leaf_c[3 * (size_t)leaf + 1];
+                ncz = J.leaf_c[3 * (size_t)leaf + 2];
+                if (lane < rl) na = J.t4[rs + lane];
+                if (lane + 32 < rl) nb = J.t4[rs + lane + 32];
             } else {
                 const unsigned rs = nrec.x;
                 if (lane < rl) {
-                    ncx = A.tx[rs + lane];
-                    ncy = A.ty[rs + lane];
-                    ncz = A.tz[rs + lane];
+                    ncx = J.tx[rs + lane];
+                    ncy = J.ty[rs + lane];
+                    ncz = J.tz[rs + lane];
                 }
             }
         };
@@ -590,9 +632,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         ws->stage64[2 * KD_RUN_MAX + lane] = ncz;
                     }
                     for (int j = lane + 32; j < rl; j += 32) {
-                        ws->stage64[j] = A.tx[rs + j];
-                        ws->stage64[KD_RUN_MAX + j] = A.ty[rs + j];
-                        ws->stage64[2 * KD_RUN_MAX + j] = A.tz[rs + j];
+                        ws->stage64[j] = J.tx[rs + j];
+                        ws->stage64[KD_RUN_MAX + j] = J.ty[rs + j];
+                        ws->stage64[2 * KD_RUN_MAX + j] = J.tz[rs + j];
                     }
                 }
             }
@@ -646,9 +688,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
 #pragma unroll
                     for (int p = 0; p < kQ; p++) {
                         const bool v = (vmask >> p) & 1;
-                        qxd[p] = v ? A.Q.x[qbase + p] : ox;
-                        qyd[p] = v ? A.Q.y[qbase + p] : oy;
-                        qzd[p] = v ? A.Q.z[qbase + p] : oz;
+                        qxd[p] = v ? J.Q.x[qbase + p] : ox;
+                        qyd[p] = v ? J.Q.y[qbase + p] : oy;
+                        qzd[p] = v ? J.Q.z[qbase + p] : oz;
                     }
                     const double *s64 = ws->stage64;
                     switch (kn) {
@@ -664,8 +706,8 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                 for (int p = 0; p < kQ; p++)
                     if ((redo >> p) & 1) {
                         const unsigned pk =
-                            exact_pass(A.tx + rs, A.ty + rs, A.tz + rs, rl, A.Q.x[qbase + p],
-                                       A.Q.y[qbase + p], A.Q.z[qbase + p], R + k0 + kb, kn);
+                            exact_pass(J.tx + rs, J.ty + rs, J.tz + rs, rl, J.Q.x[qbase + p],
+                                       J.Q.y[qbase + p], J.Q.z[qbase + p], R + k0 + kb, kn);
 #pragma unroll
                         for (int k = 0; k < 4; k++) cnt[p][k] = (pk >> (8 * k)) & 0xFF;
                     }
@@ -734,11 +776,59 @@ static float elapsed(cudaEvent_t a, cudaEvent_t b)
     return ms;
 }
 
-static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double *h_rsq, int ne,
-                       int mode, int shard, int nshards, long long *hist, kd_count_stats *stats)
+// the traversal and tile views of one (tree, query tree) job
+static JobDesc job_desc(const kd_catalog *tc, const kd_catalog *qc, unsigned long long *H)
 {
-    if (tc->device != qc->device) raise(KD_EINVAL, "tree and query catalogs on different devices");
-    check(cudaSetDevice(tc->device), "cudaSetDevice");
+    JobDesc d;
+    memset(&d, 0, sizeof d);
+    d.T.x = tc->d_x;
+    d.T.y = tc->d_y;
+    d.T.z = tc->d_z;
+    d.T.box = tc->d_box;
+    d.T.count = tc->d_ncount;
+    d.T.tf = tc->d_ntf;
+    d.T.leaf_run = tc->d_leaf_run;
+    d.T.run_start = tc->d_run_start;
+    d.T.run_len = tc->d_run_len;
+    d.T.run_tf = tc->d_run_tf;
+    d.T.D = tc->depth;
+    d.T.nleaves = tc->nleaves;
+    d.Q.x = qc->d_x;
+    d.Q.y = qc->d_y;
+    d.Q.z = qc->d_z;
+    d.Q.qf = qc->d_qf;
+    d.Q.blk_start = qc->d_blk_start;
+    d.Q.blk_len = qc->d_blk_len;
+    d.Q.blk_qf = qc->d_blk_qf;
+    d.Q.blk_box = qc->d_blk_box;
+    d.tx = tc->d_x;
+    d.ty = tc->d_y;
+    d.tz = tc->d_z;
+    d.t4 = (const float4 *)tc->d_t4;
+    d.leaf_c = tc->d_leaf_c;
+    d.hT = tc->leaf_hdiag * (1.0 + 1e-12);
+    d.H = H;
+    d.Fqe = qc->max_qf + 1;
+    d.Fte = tc->max_tf + 1;
+    return d;
+}
+
+static size_t hist_size(const kd_catalog *tc, const kd_catalog *qc, int ne)
+{
+    return (size_t)(ne + 1) * (size_t)(qc->max_qf + 1) * (size_t)(tc->max_tf + 1);
+}
+
+// Every job's query blocks (this shard's share of them) in one traversal and
+// one persistent tile launch per record batch, over a shared work counter.
+static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *const *qcs,
+                             int njobs, const double *h_rsq, int ne, int mode, int shard,
+                             int nshards, long long *const *hists, kd_count_stats *stats)
+{
+    const int device = tcs[0]->device;
+    for (int j = 0; j < njobs; j++)
+        if (tcs[j]->device != device || qcs[j]->device != device)
+            raise(KD_EINVAL, "the catalogs of a count are on different devices");
+    check(cudaSetDevice(device), "cudaSetDevice");
     init_device();
     Stream st;
     cudaStream_t s = st.s;
@@ -746,32 +836,20 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     Events ev;
     int launches = 0, tile_launches = 0;
 
-    TreeSide T;
-    T.x = tc->d_x;
-    T.y = tc->d_y;
-    T.z = tc->d_z;
-    T.box = tc->d_box;
-    T.count = tc->d_ncount;
-    T.tf = tc->d_ntf;
-    T.leaf_run = tc->d_leaf_run;
-    T.run_start = tc->d_run_start;
-    T.run_len = tc->d_run_len;
-    T.run_tf = tc->d_run_tf;
-    T.D = tc->depth;
-    T.nleaves = tc->nleaves;
-    QuerySide Q;
-    Q.x = qc->d_x;
-    Q.y = qc->d_y;
-    Q.z = qc->d_z;
-    Q.qf = qc->d_qf;
-    Q.blk_start = qc->d_blk_start;
-    Q.blk_len = qc->d_blk_len;
-    Q.blk_qf = qc->d_blk_qf;
-    Q.blk_box = qc->d_blk_box;
-
-    const int Fqe = qc->max_qf + 1, Fte = tc->max_tf + 1;
-    const size_t hsz = (size_t)(ne + 1) * Fqe * Fte;
+    // job table, histogram offsets, global block numbering
+    std::vector<size_t> hoff(njobs + 1, 0);
+    std::vector<int> hblk(njobs + 1, 0);
+    for (int j = 0; j < njobs; j++) {
+        hoff[j + 1] = hoff[j] + hist_size(tcs[j], qcs[j], ne);
+        if ((long long)hblk[j] + qcs[j]->nblocks > INT_MAX) raise(KD_EINVAL, "too many query blocks in one count");
+        hblk[j + 1] = hblk[j] + qcs[j]->nblocks;
+    }
+    const size_t hsz = hoff[njobs];
     unsigned long long *H = pool.alloc<unsigned long long>(hsz);
+    std::vector<JobDesc> hj(njobs);
+    for (int j = 0; j < njobs; j++) hj[j] = job_desc(tcs[j], qcs[j], H + hoff[j]);
+    JobDesc *jobs = pool.alloc<JobDesc>(njobs);
+    int *jblk = pool.alloc<int>(njobs + 1);
     unsigned long long *dstats = pool.alloc<unsigned long long>(8);
     int *err = pool.alloc<int>(1);
     int *work = pool.alloc<int>(1);
@@ -781,29 +859,28 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     check(cudaMemsetAsync(dstats, 0, sizeof(unsigned long long) * 8, s), "memset");
     check(cudaMemsetAsync(err, 0, sizeof(int), s), "memset");
     check(cudaMemcpyAsync(rsq, h_rsq, sizeof(double) * ne, cudaMemcpyHostToDevice, s), "H2D");
+    check(cudaMemcpyAsync(jobs, hj.data(), sizeof(JobDesc) * njobs, cudaMemcpyHostToDevice, s), "H2D");
+    check(cudaMemcpyAsync(jblk, hblk.data(), sizeof(int) * (njobs + 1), cudaMemcpyHostToDevice, s),
+          "H2D");
 
-    // this shard's query blocks, renumbered from 0
-    const int blo = (int)((long long)qc->nblocks * shard / nshards);
-    const int nb = (int)((long long)qc->nblocks * (shard + 1) / nshards) - blo;
-    Q.blk_start += blo;
-    Q.blk_len += blo;
-    Q.blk_qf += blo;
-    Q.blk_box += 6 * (size_t)blo;
+    // this shard's global blocks
+    const int NB = hblk[njobs];
+    const int G0 = (int)((long long)NB * shard / nshards);
+    const int G1 = (int)((long long)NB * (shard + 1) / nshards);
+    const int nb = G1 - G0;
     int *cnt = pool.alloc<int>(std::max(nb, 1));
     TravOut to;
     memset(&to, 0, sizeof to);
     to.count = cnt;
-    to.H = H;
-    to.Fqe = Fqe;
-    to.Fte = Fte;
     to.accepted = dstats + 2;
     to.err = err;
     if (nb > 0) {
-        k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0, nb, to);
+        k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(jobs, jblk, njobs,
+                                                                                  rsq, ne, G0, G1, to);
         launches++;
     }
     KD_LAUNCH_CHECK("k_traverse(count)");
-    std::vector<int> hcnt(nb);
+    std::vector<int> hcnt(std::max(nb, 1));
     check(cudaMemcpyAsync(hcnt.data(), cnt, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToHost, s),
           "D2H");
     int herr = 0;
@@ -811,68 +888,63 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     st.sync();
     if (herr) raise(herr, "node-pair traversal exceeded its stack");
 
-    // batches of query blocks whose tile records fit the buffer
+    // batches of global blocks whose tile records fit the buffer: up to 2^30
+    // records (16 GiB) or a quarter of the free memory, so that on a B200 a
+    // full DD + DR + RR batch of 20M-point catalogs runs as one launch
     long long total = 0;
-    for (int v : hcnt) total += v;
+    for (int i = 0; i < nb; i++) total += hcnt[i];
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
     long long cap = std::max<long long>(
-        1 << 20, std::min<long long>(256LL << 20, (long long)(freeb / 4 / sizeof(uint4))));
+        1 << 20, std::min<long long>(1LL << 30, (long long)(freeb / 4 / sizeof(uint4))));
     cap = std::min<long long>(cap, std::max<long long>(total, 1));
     uint4 *rec = pool.alloc<uint4>(cap);
     long long *off = pool.alloc<long long>(nb + 1);
-    std::vector<long long> hoff(nb + 1);
+    std::vector<long long> hoffs(nb + 1);
 
     const size_t smem = tile_smem(ne, mode);
     auto kern = mode == KD_MODE_MIXED ? k_tiles<KD_MODE_MIXED> : k_tiles<KD_MODE_FP64>;
     check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
           "smem attribute");
-    int dev = 0, nsm = 148, occ = 1;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int nsm = 148, occ = 1;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * kTileWarpsPerCta, smem),
           "occupancy");
     occ = std::max(occ, 1);
 
     float ms_trav = 0, ms_tiles = 0;
-    int b0 = 0;
+    int b0 = 0;  // shard-relative
     while (b0 < nb) {
         long long acc = 0;
         int b1 = b0;
-        hoff[0] = 0;
+        hoffs[0] = 0;
         while (b1 < nb && (b1 == b0 || acc + hcnt[b1] <= cap)) {
             acc += hcnt[b1];
             b1++;
-            hoff[b1 - b0] = acc;
+            hoffs[b1 - b0] = acc;
         }
-        check(cudaMemcpyAsync(off, hoff.data(), sizeof(long long) * (size_t)(b1 - b0 + 1),
+        check(cudaMemcpyAsync(off, hoffs.data(), sizeof(long long) * (size_t)(b1 - b0 + 1),
                               cudaMemcpyHostToDevice, s), "H2D");
         TravOut tf = to;
+        tf.count = nullptr;
         tf.off = off;
         tf.rec = rec;
         check(cudaEventRecord(ev.e[1], s), "event");
-        k_traverse<true><<<blocks_for(b1 - b0, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne,
-                                                                                      b0, b1, tf);
+        k_traverse<true><<<blocks_for(b1 - b0, kTravWarps), 32 * kTravWarps, 0, s>>>(
+            jobs, jblk, njobs, rsq, ne, G0 + b0, G0 + b1, tf);
         launches++;
         KD_LAUNCH_CHECK("k_traverse(fill)");
         check(cudaEventRecord(ev.e[2], s), "event");
         TileArgs ta;
-        ta.tx = tc->d_x;
-        ta.ty = tc->d_y;
-        ta.tz = tc->d_z;
-        ta.t4 = (const float4 *)tc->d_t4;
-        ta.leaf_c = tc->d_leaf_c;
-        ta.hT = tc->leaf_hdiag * (1.0 + 1e-12);
-        ta.Q = Q;
+        ta.jobs = jobs;
+        ta.jblk = jblk;
+        ta.njobs = njobs;
         ta.rsq = rsq;
         ta.ne = ne;
-        ta.b0 = b0;
-        ta.b1 = b1;
+        ta.g0 = G0 + b0;
+        ta.g1 = G0 + b1;
         ta.off = off;
         ta.rec = rec;
-        ta.H = H;
-        ta.Fqe = Fqe;
-        ta.Fte = Fte;
         ta.work = work;
         ta.stats = dstats;
         check(cudaMemsetAsync(work, 0, sizeof(int), s), "memset");
@@ -889,7 +961,7 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
         b0 = b1;
     }
     check(cudaEventRecord(ev.e[4], s), "event");
-    std::vector<unsigned long long> hh(hsz);
+    std::vector<unsigned long long> hh(std::max<size_t>(hsz, 1));
     unsigned long long hs[8];
     check(cudaMemcpyAsync(hh.data(), H, sizeof(unsigned long long) * hsz, cudaMemcpyDeviceToHost, s),
           "D2H");
@@ -897,7 +969,8 @@ static void count_impl(const kd_catalog *tc, const kd_catalog *qc, const double 
     check(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
     st.sync();
     if (herr) raise(herr, "node-pair traversal exceeded its stack");
-    for (size_t i = 0; i < hsz; i++) hist[i] = (long long)hh[i];
+    for (int j = 0; j < njobs; j++)
+        for (size_t i = hoff[j]; i < hoff[j + 1]; i++) hists[j][i - hoff[j]] = (long long)hh[i];
     if (stats) {
         stats->pairs_tested = (long long)hs[0];
         stats->pairs_rechecked = (long long)hs[1];
@@ -1014,28 +1087,6 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
     unsigned char *base = static_scratch(tc->device);
     const cudaStream_t s = 0;  // legacy default stream: nothing is created
 
-    TreeSide T;
-    T.x = tc->d_x;
-    T.y = tc->d_y;
-    T.z = tc->d_z;
-    T.box = tc->d_box;
-    T.count = tc->d_ncount;
-    T.tf = tc->d_ntf;
-    T.leaf_run = tc->d_leaf_run;
-    T.run_start = tc->d_run_start;
-    T.run_len = tc->d_run_len;
-    T.run_tf = tc->d_run_tf;
-    T.D = tc->depth;
-    T.nleaves = tc->nleaves;
-    QuerySide Q;
-    Q.x = qc->d_x;
-    Q.y = qc->d_y;
-    Q.z = qc->d_z;
-    Q.qf = qc->d_qf;
-    Q.blk_start = qc->d_blk_start;
-    Q.blk_len = qc->d_blk_len;
-    Q.blk_qf = qc->d_blk_qf;
-    Q.blk_box = qc->d_blk_box;
     const int nb = qc->nblocks;
     const int Fqe = qc->max_qf + 1, Fte = tc->max_tf + 1;
     const size_t hsz = (size_t)(ne + 1) * Fqe * Fte;
@@ -1048,6 +1099,8 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
         return p;
     };
     auto *H = (unsigned long long *)take(sizeof(unsigned long long) * hsz);
+    auto *job = (JobDesc *)take(sizeof(JobDesc));
+    auto *jblk = (int *)take(sizeof(int) * 2);
     auto *misc = (unsigned long long *)take(sizeof(unsigned long long) * 8);  // stats
     auto *err = (int *)take(sizeof(int) * 4);  // err, work, b1
     auto *rsq = (double *)take(sizeof(double) * KD_MAX_EDGES);
@@ -1072,19 +1125,20 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
     check(cudaMemsetAsync(cnt, 0, sizeof(long long) * ((size_t)nb + 1), s), "memset");
     check(cudaMemcpyAsync(rsq, rsq_sorted, sizeof(double) * ne, cudaMemcpyHostToDevice, s), "H2D");
     check(cudaMemcpyAsync(eo, edge_of, sizeof(int) * nradii, cudaMemcpyHostToDevice, s), "H2D");
+    const JobDesc hjob = job_desc(tc, qc, H);
+    const int hjblk[2] = {0, nb};
+    check(cudaMemcpyAsync(job, &hjob, sizeof hjob, cudaMemcpyHostToDevice, s), "H2D");
+    check(cudaMemcpyAsync(jblk, hjblk, sizeof hjblk, cudaMemcpyHostToDevice, s), "H2D");
 
     // tile counts per block (the traversal writes int counts; widen in place)
     TravOut to;
     memset(&to, 0, sizeof to);
     to.count = (int *)off;  // int counts, staged in off's storage
-    to.H = H;
-    to.Fqe = Fqe;
-    to.Fte = Fte;
     to.accepted = misc + 2;
     to.err = err;
     if (nb > 0)
-        k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne, 0,
-                                                                                  nb, to);
+        k_traverse<false><<<blocks_for(nb, kTravWarps), 32 * kTravWarps, 0, s>>>(job, jblk, 1, rsq,
+                                                                                  ne, 0, nb, to);
     KD_LAUNCH_CHECK("k_traverse(count)");
     k_gather_widen<<<blocks_for(nb, 256), 256, 0, s>>>((const int *)off, nb, cnt);
     check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cnt, off, nb + 1, s), "scan");
@@ -1110,26 +1164,19 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
         tf.count = nullptr;
         tf.off = rel;
         tf.rec = rec;
-        k_traverse<true><<<blocks_for(b1 - b0, kTravWarps), 32 * kTravWarps, 0, s>>>(T, Q, rsq, ne,
-                                                                                      b0, b1, tf);
+        k_traverse<true><<<blocks_for(b1 - b0, kTravWarps), 32 * kTravWarps, 0, s>>>(job, jblk, 1,
+                                                                                      rsq, ne, b0, b1, tf);
         KD_LAUNCH_CHECK("k_traverse(fill)");
         TileArgs ta;
-        ta.tx = tc->d_x;
-        ta.ty = tc->d_y;
-        ta.tz = tc->d_z;
-        ta.t4 = (const float4 *)tc->d_t4;
-        ta.leaf_c = tc->d_leaf_c;
-        ta.hT = tc->leaf_hdiag * (1.0 + 1e-12);
-        ta.Q = Q;
+        ta.jobs = job;
+        ta.jblk = jblk;
+        ta.njobs = 1;
         ta.rsq = rsq;
         ta.ne = ne;
-        ta.b0 = b0;
-        ta.b1 = b1;
+        ta.g0 = b0;
+        ta.g1 = b1;
         ta.off = rel;
         ta.rec = rec;
-        ta.H = H;
-        ta.Fqe = Fqe;
-        ta.Fte = Fte;
         ta.work = err + 1;
         ta.stats = misc;
         check(cudaMemsetAsync(err + 1, 0, sizeof(int), s), "memset");
@@ -1184,9 +1231,9 @@ extern "C" int kdg_set_device(int device)
     return KD_OK;
 }
 
-extern "C" int kdg_count(const kd_catalog *tree, const kd_catalog *query, const double *rsq,
-                         int ne, int mode, int shard, int nshards, long long *hist,
-                         kd_count_stats *stats)
+extern "C" int kdg_count_batch(const kd_catalog *const *trees, const kd_catalog *const *queries,
+                               int njobs, const double *rsq, int ne, int mode, int shard,
+                               int nshards, long long *const *hists, kd_count_stats *stats)
 {
     if (nshards < 1 || shard < 0 || shard >= nshards) {
         kd_set_error(KD_EINVAL, "shard %d of %d", shard, nshards);
@@ -1196,11 +1243,22 @@ extern "C" int kdg_count(const kd_catalog *tree, const kd_catalog *query, const 
         kd_set_error(KD_EINVAL, "between 1 and %d distinct radii per count", KD_MAX_EDGES);
         return KD_EINVAL;
     }
+    if (njobs < 1) {
+        kd_set_error(KD_EINVAL, "a batch needs at least one job");
+        return KD_EINVAL;
+    }
     try {
-        kd::count_impl(tree, query, rsq, ne, mode, shard, nshards, hist, stats);
+        kd::count_batch_impl(trees, queries, njobs, rsq, ne, mode, shard, nshards, hists, stats);
         return KD_OK;
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);
         return e.code;
     }
+}
+
+extern "C" int kdg_count(const kd_catalog *tree, const kd_catalog *query, const double *rsq,
+                         int ne, int mode, int shard, int nshards, long long *hist,
+                         kd_count_stats *stats)
+{
+    return kdg_count_batch(&tree, &query, 1, rsq, ne, mode, shard, nshards, &hist, stats);
 }

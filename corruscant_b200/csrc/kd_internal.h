@@ -124,6 +124,14 @@ int kdg_count(const kd_catalog *tree, const kd_catalog *query,
               const double *rsq, int ne, int mode, int shard, int nshards,
               long long *hist, kd_count_stats *stats);
 
+/* kdg_count for njobs (trees[j], queries[j]) pairs at once: all their query
+ * blocks are numbered consecutively (job after job) and counted by one
+ * traversal and one persistent tile launch per record batch; hists[j] has
+ * kdg_count's layout for job j.  shard/nshards split the global blocks. */
+int kdg_count_batch(const kd_catalog *const *trees, const kd_catalog *const *queries,
+                    int njobs, const double *rsq, int ne, int mode, int shard, int nshards,
+                    long long *const *hists, kd_count_stats *stats);
+
 /* Coordinates (libcoords). */
 int kdg_radec2cart(const double *ra, const double *dec, const double *dist,
                    double *xyz, int n);

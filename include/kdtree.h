@@ -135,6 +135,26 @@ int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii,
                          int nradii, int mode, int shard, int nshards,
                          long long *out, kd_count_stats *stats);
 
+/* kd_count_radii for njobs (trees[j], queries[j]) pairs sharing the radii
+ * and mode, e.g. DD, DR and RR of an autocorrelation (clustering.py:218-230)
+ * or the counts of many catalogs against one random catalog.  The query
+ * blocks of all jobs are numbered consecutively and counted by one node-pair
+ * traversal and one persistent tile launch over a shared work queue, so small
+ * jobs do not each pay for launches and an underfilled GPU.  out receives,
+ * job after job, each job's kd_count_radii result: nradii * Fq_j * Ft_j
+ * counts (Fq_j = queries[j].num_fields, Ft_j = trees[j].num_fields).  stats
+ * (may be NULL) totals the batch. */
+int kd_count_batch(const kdtree_t *trees, const kdtree_t *queries, int njobs,
+                   const double *radii, int nradii, int mode, long long *out,
+                   kd_count_stats *stats);
+
+/* One shard of kd_count_batch: blocks [nb*shard/nshards, nb*(shard+1)/nshards)
+ * of the batch's nb global query blocks.  Summing out over all shards gives
+ * kd_count_batch's result exactly. */
+int kd_count_batch_shard(const kdtree_t *trees, const kdtree_t *queries, int njobs,
+                         const double *radii, int nradii, int mode, int shard,
+                         int nshards, long long *out, kd_count_stats *stats);
+
 /* kd_count_radii for callers that cannot allocate device memory while they
  * count: a service whose device memory is owned by a fixed-budget pool, a
  * host that forbids cudaMalloc because it synchronizes the whole device and
