@@ -1,35 +1,54 @@
 #!/usr/bin/env python
 """Benchmark of the pair-counting hot path on one or more B200s.
 
-Workload (the clustered 3-D autocorrelation the headline metric is quoted on):
+Default workload (--workload clustered3d, the clustered 3-D autocorrelation
+the headline metric is quoted on):
   data     1,000,000 points, Neyman-Scott: 10,000 uniform parents in the unit
            cube x 100 children with N(0, 0.005^2) isotropic offsets, wrapped
            periodically (numpy seed 11)
   randoms  20,000,000 uniform points in the unit cube (numpy seed 12)
   edges    21 radii logspace(-3, -1, 21) (20 bins)
   fields   64 jackknife fields on a 4x4x4 grid: 16*floor(4x)+4*floor(4y)+floor(4z)
-Synthetic inputs of the named shapes (no dataset is involved).
+Other workloads, measured the same way (seeded synthetic inputs of the named
+shapes; no dataset is involved):
+  angular  2,000,000 (RA, DEC) points in RA 0-90 deg, DEC -10..60 deg uniform
+           in sin DEC, half of them in Gaussian blobs (sigma 0.05 deg, tangent
+           plane) around 20,000 centres; 20,000,000 uniform randoms; 16 edges
+           theta = logspace(-3, log10 2, 16) deg as chords; 100 fields (10 x 10
+           data quantiles in RA x sin DEC); DD + DR + RR
+  mocks    128 Neyman-Scott catalogs (N/100 parents, sigma 0.005) with sizes
+           log-uniform in 20,000..500,000, one shared 5,000,000-point uniform
+           random catalog; 13 edges logspace(log10 2e-3, -1, 13); 16 fields
+           4*floor(4x)+floor(4y); DD_i and D_iR for every catalog plus RR:
+           257 counts in one batch
+  lattice  4,000,000 data points on the 1/1024 lattice with 10% of the rows
+           replaced by copies of other rows, 4,000,000 randoms on the same
+           lattice; 30 edges sqrt(k)/1024 for 30 log-spaced integers k in
+           [1, 10486] (many pairs exactly on an edge); 27 fields 3x3x3; both
+           cross counts (DR and RD); the FP64 recheck rate is reported
 
-A step is DD + DR + RR for all 21 edges: one kd_count_batch call on prebuilt
-trees, inputs resident in HBM.  value = pairs tested per second, all ranks,
-with the mixed FP32 + FP64-recheck counter; the plain FP64 counter is timed
-on the same steps.  e2e = the same pairs per second through the C ABI from
-host buffers: tree_construct of both catalogs (H2D of the points, node arrays
-back to the host), the batched count, results read back, every step.  Also
-reported: the FP64 form against a measured DGEMM peak, the all-pairs-
-equivalent rate (Nd^2 + Nd Nr + Nr^2 per step over the step time) and an
-FP32-pipe model of the binning (FMA lane-ops per pair from the measured
-active edges per pair).
+A step is every count of the workload for all edges: one kd_count_batch call
+on prebuilt trees, inputs resident in HBM.  value = pairs tested per second,
+all ranks, with the mixed FP32 + FP64-recheck counter; the plain FP64 counter
+is timed on the same steps.  e2e = the same pairs per second through the C ABI
+from host buffers: tree_construct of every catalog (H2D of the points, node
+arrays back to the host; for the angular workload the RA/DEC conversion too),
+the batched count, results read back, every step.  Also reported: the FP64
+form against a measured DGEMM peak, the all-pairs-equivalent rate (sum of
+Nq * Nt over the counts, per step time) and an FP32-pipe model of the binning
+(FMA lane-ops per pair from the measured active edges per pair).
 
 --gpus N (torchrun): every rank builds the trees and counts its 1/N share of
-the batch's query blocks (kd_count_batch_shard); the per-rank counts are summed with
-one all-reduce and checked against rank 0's expectations.  Total work is
-fixed: scaling "strong".
+the batch's query blocks (kd_count_batch_shard); the per-rank counts are
+summed with one all-reduce and checked across modes.  Total work is fixed:
+scaling "strong".
 
 --impl reference: the reference's own CPU path (oracle/_ref/libkdtree.so,
 compiled from the reference sources) driven like clustering._autocorr, one
 pair_count call per edge, all host threads, on a bounded seeded subset of the
-queries against the full trees; rank 0 only.
+queries of every count against the full trees; rank 0 only.  The same leg,
+run as this arm's cpu_baseline, also checks the GPU's counts for those query
+subsets against the reference's.
 """
 import argparse
 import json
@@ -46,29 +65,169 @@ sys.path.insert(0, HERE)
 
 METRIC = "pairs tested/s, exact counts: FP32+FP64-recheck vs plain FP64 on B200; CPU ref"
 UNIT = "pairs/s"
-N_DATA, N_PARENTS, SIGMA = 1_000_000, 10_000, 0.005
-N_RAND = 20_000_000
-N_FIELDS = 64
 FLOP_PER_PAIR = 8  # 3 subtractions, 1 multiply, 2 fused multiply-adds per distance
-WORKLOAD = ("3D clustered autocorr: 1M Neyman-Scott data (10k parents x 100, sigma 0.005, "
-            "periodic), 20M uniform randoms, 21 edges logspace(-3,-1), 64 fields 4x4x4; "
-            "a step is DD+DR+RR over all edges")
+
+# ---------------------------------------------------------------- workloads
 
 
-def make_workload(scale=1.0):
-    nd, nr, npar = int(N_DATA * scale), int(N_RAND * scale), max(1, int(N_PARENTS * scale))
-    rs = np.random.RandomState(11)
-    parents = rs.rand(npar, 3)
-    data = (np.repeat(parents, nd // npar + 1, axis=0)[:nd] +
-            rs.normal(0.0, SIGMA, (nd, 3))) % 1.0
+class Workload:
+    """Catalogs (name -> points (n,3) f64, fields int32 or None, field count),
+    counts (name, tree catalog, query catalog) and radii of one benchmark.
+    radec: for catalogs given on the sky, name -> (ra, dec) in degrees, from
+    which the points were computed."""
+
+    def __init__(self, name, description, catalogs, jobs, radii, data, cpu_queries,
+                 radec=None):
+        self.name, self.description = name, description
+        self.catalogs, self.jobs, self.radii = catalogs, jobs, np.asarray(radii, np.float64)
+        self.data, self.cpu_queries, self.radec = data, cpu_queries, radec or {}
+
+
+def _neyman_scott(rs, n, nparents, sigma):
+    parents = rs.rand(nparents, 3)
+    return (np.repeat(parents, n // nparents + 1, axis=0)[:n] +
+            rs.normal(0.0, sigma, (n, 3))) % 1.0
+
+
+def wl_clustered3d(scale=1.0):
+    nd, nr, npar = int(1_000_000 * scale), int(20_000_000 * scale), max(1, int(10_000 * scale))
+    data = _neyman_scott(np.random.RandomState(11), nd, npar, 0.005)
     rand = np.random.RandomState(12).rand(nr, 3)
 
     def fields(p):
         return (16 * np.floor(4 * p[:, 0]) + 4 * np.floor(4 * p[:, 1]) +
                 np.floor(4 * p[:, 2])).astype(np.int32)
-    radii = np.logspace(-3, -1, 21)
-    return (np.ascontiguousarray(data), fields(data), np.ascontiguousarray(rand), fields(rand),
-            radii)
+    return Workload(
+        "clustered3d",
+        ("3D clustered autocorr: 1M Neyman-Scott data (10k parents x 100, sigma 0.005, "
+         "periodic), 20M uniform randoms, 21 edges logspace(-3,-1), 64 fields 4x4x4; "
+         "a step is DD+DR+RR over all edges"),
+        {"D": (np.ascontiguousarray(data), fields(data), 64),
+         "R": (np.ascontiguousarray(rand), fields(rand), 64)},
+        [("DD", "D", "D"), ("DR", "R", "D"), ("RR", "R", "R")],
+        np.logspace(-3, -1, 21), "synthetic (seeded Neyman-Scott data and uniform randoms)", 4000)
+
+
+def _patch_uniform(rs, n, ra_lim=(0.0, 90.0), dec_lim=(-10.0, 60.0)):
+    ra = rs.uniform(ra_lim[0], ra_lim[1], n)
+    s0, s1 = np.sin(np.radians(dec_lim[0])), np.sin(np.radians(dec_lim[1]))
+    dec = np.degrees(np.arcsin(rs.uniform(s0, s1, n)))
+    return ra, dec
+
+
+def _blobs(rs, ncentres, per, sigma_deg, ra_lim=(0.0, 90.0), dec_lim=(-10.0, 60.0)):
+    """Gaussian blobs in tangent-plane offsets (gnomonic projection around
+    each centre); points that fall outside the patch are drawn again."""
+    cra, cdec = _patch_uniform(rs, ncentres, ra_lim, dec_lim)
+    a0 = np.radians(np.repeat(cra, per))
+    d0 = np.radians(np.repeat(cdec, per))
+    ra = np.empty(a0.size)
+    dec = np.empty(a0.size)
+    todo = np.arange(a0.size)
+    while todo.size:
+        x, y = (rs.normal(0.0, np.radians(sigma_deg), (2, todo.size)))
+        rho = np.hypot(x, y)
+        c = np.arctan(rho)
+        rho = np.where(rho == 0, 1.0, rho)
+        sd = np.cos(c) * np.sin(d0[todo]) + y * np.sin(c) * np.cos(d0[todo]) / rho
+        d = np.arcsin(np.clip(sd, -1, 1))
+        a = a0[todo] + np.arctan2(x * np.sin(c), rho * np.cos(d0[todo]) * np.cos(c) -
+                                  y * np.sin(d0[todo]) * np.sin(c))
+        a, d = np.degrees(a), np.degrees(d)
+        ok = (a >= ra_lim[0]) & (a < ra_lim[1]) & (d >= dec_lim[0]) & (d < dec_lim[1])
+        ra[todo[ok]], dec[todo[ok]] = a[ok], d[ok]
+        todo = todo[~ok]
+    return ra, dec
+
+
+def wl_angular(scale=1.0):
+    from corruscant_b200.twopoint import angular
+    rs = np.random.RandomState(14)
+    nb, nc, nr = int(1_000_000 * scale), max(1, int(20_000 * scale)), int(20_000_000 * scale)
+    ra_b, dec_b = _patch_uniform(rs, nb)
+    ra_c, dec_c = _blobs(rs, nc, 50, 0.05)
+    ra_d, dec_d = np.concatenate([ra_b, ra_c]), np.concatenate([dec_b, dec_c])
+    ra_r, dec_r = _patch_uniform(np.random.RandomState(15), nr)
+    # 100 fields: 10 x 10 quantile cells of the data in RA x sin DEC
+    qs = np.linspace(0, 1, 11)[1:-1]
+    e_ra, e_sd = np.quantile(ra_d, qs), np.quantile(np.sin(np.radians(dec_d)), qs)
+
+    def fields(ra, dec):
+        return (10 * np.searchsorted(e_ra, ra, side="right") +
+                np.searchsorted(e_sd, np.sin(np.radians(dec)), side="right")).astype(np.int32)
+    theta = np.logspace(-3, np.log10(2.0), 16)
+    return Workload(
+        "angular",
+        ("angular w(theta) autocorr: 2M (RA,DEC) points in RA 0-90, DEC -10..60 (uniform in "
+         "sin DEC), half in Gaussian blobs (sigma 0.05 deg) around 20k centres; 20M uniform "
+         "randoms; 16 theta edges logspace(-3,log10 2) deg as chords; 100 quantile fields; "
+         "a step is DD+DR+RR over all edges"),
+        {"D": (angular.cartesian(ra_d, dec_d), fields(ra_d, dec_d), 100),
+         "R": (angular.cartesian(ra_r, dec_r), fields(ra_r, dec_r), 100)},
+        [("DD", "D", "D"), ("DR", "R", "D"), ("RR", "R", "R")],
+        angular.chord(theta), "synthetic (seeded sky patch: uniform + Gaussian blobs)", 4000,
+        radec={"D": (ra_d, dec_d), "R": (ra_r, dec_r)})
+
+
+def wl_mocks(scale=1.0):
+    rs = np.random.RandomState(16)
+    sizes = np.exp(rs.uniform(np.log(20_000), np.log(500_000), 128))
+    sizes = np.maximum(1, (sizes * scale).astype(np.int64))
+
+    def fields(p):
+        return (4 * np.floor(4 * p[:, 0]) + np.floor(4 * p[:, 1])).astype(np.int32)
+    cats, jobs = {}, []
+    for i, n in enumerate(sizes):
+        p = _neyman_scott(rs, int(n), max(1, int(n) // 100), 0.005)
+        cats["M%03d" % i] = (np.ascontiguousarray(p), fields(p), 16)
+    rand = np.random.RandomState(17).rand(int(5_000_000 * scale), 3)
+    cats["R"] = (rand, fields(rand), 16)
+    for i in range(len(sizes)):
+        m = "M%03d" % i
+        jobs.append(("DD%03d" % i, m, m))
+        jobs.append(("DR%03d" % i, "R", m))
+    jobs.append(("RR", "R", "R"))
+    return Workload(
+        "mocks",
+        ("batched mocks: 128 Neyman-Scott catalogs, sizes log-uniform 20k..500k, each with "
+         "its DD and its count against one shared 5M uniform random catalog, plus RR (257 "
+         "counts in one batch); 13 edges logspace(log10 2e-3,-1); 16 fields 4x4 in x,y"),
+        cats, jobs, np.logspace(np.log10(2e-3), -1, 13),
+        "synthetic (seeded Neyman-Scott catalogs and uniform randoms)", 500)
+
+
+def wl_lattice(scale=1.0):
+    n = int(4_000_000 * scale)
+    rs = np.random.RandomState(18)
+    data = rs.randint(0, 1024, (n, 3)) / 1024.0
+    dup = rs.rand(n) < 0.10
+    data[dup] = data[rs.randint(0, n, int(dup.sum()))]
+    rand = np.random.RandomState(19).randint(0, 1024, (n, 3)) / 1024.0
+
+    def fields(p):
+        return (9 * np.floor(3 * p[:, 0]) + 3 * np.floor(3 * p[:, 1]) +
+                np.floor(3 * p[:, 2])).astype(np.int32)
+    k = np.unique(np.round(np.geomspace(1, 10486, 32)).astype(np.int64))  # 30 distinct
+    return Workload(
+        "lattice",
+        ("exactness stress cross-correlation: 4M points on the 1/1024 lattice with 10% "
+         "duplicated rows, 4M lattice randoms, 30 edges sqrt(k)/1024 (k log-spaced in "
+         "[1,10486]), 27 fields 3x3x3; a step is DR+RD over all edges"),
+        {"D": (np.ascontiguousarray(data), fields(data), 27),
+         "R": (np.ascontiguousarray(rand), fields(rand), 27)},
+        [("DR", "R", "D"), ("RD", "D", "R")],
+        np.sqrt(k.astype(np.float64)) / 1024.0, "synthetic (seeded lattice points)", 4000)
+
+
+WORKLOADS = {"clustered3d": wl_clustered3d, "angular": wl_angular, "mocks": wl_mocks,
+             "lattice": wl_lattice}
+
+
+def make_workload(scale=1.0):
+    """The default workload as (data, data fields, randoms, random fields, radii)."""
+    w = wl_clustered3d(scale)
+    (d, fd, _), (r, fr, _) = w.catalogs["D"], w.catalogs["R"]
+    return d, fd, r, fr, w.radii
 
 
 # ----------------------------------------------------------------- helpers
@@ -210,27 +369,39 @@ class Dist:
 
 # ------------------------------------------------------------------ my arm
 
+def _build_all(N, w, convert=False):
+    """Trees of every catalog; with convert, sky catalogs are converted from
+    RA/DEC on the host first (the e2e path)."""
+    from corruscant_b200.twopoint import angular
+    trees = {}
+    for name, (pts, f, nf) in w.catalogs.items():
+        if convert and name in w.radec:
+            pts = angular.cartesian(*w.radec[name])
+        trees[name] = N.build_tree(pts, f, nf)
+    return trees
+
+
 def run_mine(args):
     from corruscant_b200 import _native as N
     D = Dist()
     N.set_device(D.local)
-    data, fd, rand, fr, radii = make_workload(args.scale)
+    w = WORKLOADS[args.workload](args.scale)
+    radii = w.radii
     t0 = time.perf_counter()
-    td = N.build_tree(data, fd, N_FIELDS)
-    tr = N.build_tree(rand, fr, N_FIELDS)
+    trees = _build_all(N, w)
     build_s = time.perf_counter() - t0
-    names = ("DD", "DR", "RR")
-    jobs = [(td, td), (tr, td), (tr, tr)]
+    names = [j for j, _, _ in w.jobs]
+    jobs = [(trees[t], trees[q]) for _, t, q in w.jobs]
 
     def step(mode):
-        # DD, DR and RR in one device batch (kd_count_batch): one traversal
-        # and one persistent tile launch over all three counts' query blocks
+        # every count of the workload in one device batch (kd_count_batch):
+        # one traversal and one persistent tile launch over all their blocks
         outs, stats = N.count_batch(jobs, radii, mode=mode, with_stats=True, shard=D.rank,
                                     nshards=D.world)
         return dict(zip(names, outs)), stats
 
-    def timed(mode, k, w):
-        for _ in range(w):
+    def timed(mode, k, wu):
+        for _ in range(wu):
             step(mode)
         D.barrier()
         acc = dict(dev_ms=0.0, pairs=0, launches=0, tile_launches=0, tiles_ms=0.0, rechecked=0,
@@ -264,23 +435,25 @@ def run_mine(args):
     exact = all(np.array_equal(tot_m[k], tot_f[k]) for k in tot_m)
 
     # e2e through the C ABI from host buffers, every step
-    N.destroy(td)
-    N.destroy(tr)
+    for t in trees.values():
+        N.destroy(t)
     e2e_pairs, e2e_wall = 0, 0.0
-    h2d = data.nbytes + fd.nbytes + rand.nbytes + fr.nbytes
+    h2d = 0
+    for name, (pts, f, _) in w.catalogs.items():
+        h2d += (2 * 8 * len(pts) if name in w.radec else pts.nbytes) + (f.nbytes if f is not None else 0)
     d2h = 0
     for it in range(1 + args.steps):
         D.barrier()
         t0 = time.perf_counter()
-        a = N.build_tree(data, fd, N_FIELDS)
-        b = N.build_tree(rand, fr, N_FIELDS)
-        _, s = N.count_batch([(a, a), (b, a), (b, b)], radii, with_stats=True, shard=D.rank,
-                             nshards=D.world)
+        tt = _build_all(N, w, convert=True)
+        _, s = N.count_batch([(tt[t], tt[q]) for _, t, q in w.jobs], radii, with_stats=True,
+                             shard=D.rank, nshards=D.world)
         p = s["pairs_tested"]
         dt = time.perf_counter() - t0
-        d2h = 40 * (a.memsize + b.memsize) + 3 * 8 * len(radii) * N_FIELDS * N_FIELDS
-        N.destroy(a)
-        N.destroy(b)
+        d2h = 40 * sum(t.memsize for t in tt.values()) + 8 * len(radii) * sum(
+            tt[t].num_fields * tt[q].num_fields for _, t, q in w.jobs)
+        for t in tt.values():
+            N.destroy(t)
         if it > 0:  # the first iteration warms the allocator
             e2e_pairs += p
             e2e_wall += dt
@@ -295,7 +468,7 @@ def run_mine(args):
 
     if D.rank == 0:
         value = pairs / dev_s
-        # the dominant kernel: k_tiles, one launch per step (DD+DR+RR batch)
+        # the dominant kernel: k_tiles, one launch per step (the whole batch)
         launch_pairs = mixed["pairs"] / max(1, mixed["tile_launches"])
         launch_ms = mixed["tiles_ms"] / max(1, mixed["tile_launches"])
         achieved = launch_pairs * FLOP_PER_PAIR / (launch_ms * 1e-3) / 1e12
@@ -304,9 +477,11 @@ def run_mine(args):
                     "frac": (achieved / peak) if peak else None,
                     "traffic": TILE_TRAFFIC_PER_PAIR * launch_pairs
                     if TILE_TRAFFIC_PER_PAIR else None,
-                    "kernel": "k_tiles<mixed> (one launch: DD+DR+RR batch)",
+                    "kernel": "k_tiles<mixed> (one launch: the step's whole batch)",
                     "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off",
                     "flop_per_pair": FLOP_PER_PAIR}
+        if TILE_TRAFFIC_PER_PAIR:
+            roofline["traffic_source"] = TILE_TRAFFIC_SOURCE
         # FP32-pipe model of the binning itself: per pair 3 FMA lane-ops for
         # the distance and 3 per active edge (ramp, count, band check)
         kbar = mixed["edge_pairs"] / max(1, mixed["pairs"])
@@ -325,18 +500,22 @@ def run_mine(args):
                          "unit": "TFLOP/s", "frac": (f_achieved / peak64) if peak64 else None,
                          "kernel": "k_tiles<fp64>",
                          "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"}
-        nd, nr = len(data), len(rand)
-        all_pairs = float(nd) * nd + float(nr) * nd + float(nr) * nr
+        sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
+        all_pairs = float(sum(sizes[q] * sizes[t] for _, t, q in w.jobs))
+        cfg = {"workload": w.description, "counts": len(w.jobs), "edges": len(radii),
+               "parallelism": f"query blocks sharded over {D.world} GPU(s)",
+               "l2": "inputs larger than L2 (tree points stream from HBM each step)"}
+        if len(sizes) <= 4:
+            cfg["catalogs"] = sizes
+        else:
+            cfg["catalog_points_total"] = int(sum(sizes.values()))
+            cfg["catalogs"] = len(sizes)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev_s / args.steps * 1e3, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
-            "data": "synthetic (seeded Neyman-Scott data and uniform randoms)",
-            "config": {"workload": WORKLOAD, "n_data": len(data), "n_rand": len(rand),
-                       "edges": len(radii), "fields": N_FIELDS,
-                       "parallelism": f"query blocks sharded over {D.world} GPU(s)",
-                       "l2": "inputs larger than L2 (20M tree points: 640 MB FP64 + 320 MB FP32)"},
+            "data": w.data, "config": cfg,
             "fp64_form": {"value": fpairs / fdev_s, "ms_per_step": fdev_s / args.steps * 1e3,
                           "dtype": "f64", "roofline": fp64_roofline},
             "all_pairs_equivalent_per_s": all_pairs / (dev_s / args.steps),
@@ -344,6 +523,7 @@ def run_mine(args):
             "mixed_over_fp64": (pairs / dev_s) / (fpairs / fdev_s),
             "counts_exact_mixed_vs_fp64": bool(exact),
             "recheck_rate": rechecked / max(1, pairs),
+            "pairs_rechecked_per_step": rechecked / args.steps,
             "build_s": build_s,
             "roofline": roofline,
             "e2e": {"value": e_pairs / e_wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -352,91 +532,129 @@ def run_mine(args):
             "gpu_launches": int(mixed["launches"]),
         }
         if D.world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(data, fd, rand, fr, radii,
-                                                n_queries=args.cpu_queries)
+            line["cpu_baseline"] = cpu_baseline(w, n_queries=args.cpu_queries, gpu=N)
         print(json.dumps(line), flush=True)
     D.close()
 
 
-# Per-pair DRAM traffic of the tile kernel from an ncu capture (bytes read +
-# written by k_tiles over pairs tested; profiles/k_tiles_config2.md), scaled
-# to a full RR launch by its pairs.
+# Per-pair DRAM traffic of the tile kernel (dram bytes read + written by one
+# k_tiles launch over the pairs it tested), from the ncu capture of the
+# clustered workload at scale 0.3 summarised in profiles/, scaled to a full
+# launch by its pairs: the traffic is mostly the tile records, whose number
+# grows with the pairs.
 TILE_TRAFFIC_PER_PAIR = None
+TILE_TRAFFIC_SOURCE = None
 
 
 # ------------------------------------------------------- reference (CPU) arm
 
-def _ref_sample(rs, n, k):
-    return np.sort(rs.choice(n, size=min(k, n), replace=False))
-
-
-def cpu_baseline(data, fd, rand, fr, radii, n_queries=4000, steps=1, warmup=0):
+def cpu_baseline(w, n_queries=None, steps=1, warmup=0, gpu=None):
     """The reference's pthreaded CPU path (oracle/_ref, compiled from its
-    sources) on a seeded query subset of DD, DR and RR against the full
-    trees, one pair_count call per edge like clustering._autocorr.  Its
-    "pairs tested" are the node distance evaluations of its traversal,
-    counted by the oracle over the same node arrays."""
+    sources) on a seeded query subset of every count against the full trees,
+    one pair_count call per edge like clustering._autocorr.  Its "pairs
+    tested" are the node distance evaluations of its traversal, counted by
+    the oracle over the same node arrays.  With gpu (the corruscant_b200
+    native module) the GPU's counts for the same query subsets are compared
+    with the reference's."""
     from oracle import oracle as O
     if not O.ref_available():
         return {"value": None, "unit": UNIT, "kind": "reference",
                 "unavailable": "oracle/_ref not built (make -C oracle ref)"}
     R = O.RefLib()
     cores = os.cpu_count() or 1
-    td = R.build(data, fd, N_FIELDS)
-    tr = R.build(rand, fr, N_FIELDS)
+    nq_max = n_queries or w.cpu_queries
+    # the reference converts sky catalogs with its own coordinate library
+    pts = {}
+    coords_equal = True
+    for name, (p, _, _) in w.catalogs.items():
+        if name in w.radec:
+            pts[name] = R.radec2cart64(*w.radec[name])
+            coords_equal &= bool(np.array_equal(pts[name].view(np.int64), p.view(np.int64)))
+        else:
+            pts[name] = p
+    used = sorted({t for _, t, _ in w.jobs})
+    rtrees = {n: R.build(pts[n], w.catalogs[n][1], w.catalogs[n][2]) for n in used}
     rs = np.random.RandomState(13)
-    sd = _ref_sample(rs, len(data), n_queries)
-    sr = _ref_sample(rs, len(rand), n_queries)
-    jobs = (("DD", td, data[sd], fd[sd]), ("DR", tr, data[sd], fd[sd]),
-            ("RR", tr, rand[sr], fr[sr]))
-    nthreads = max(1, min(cores, n_queries // 20))  # pair_count exits above n/20
-    per_type = {name: [] for name, _, _, _ in jobs}
+    samples, skipped = [], []
+    for name, t, q in w.jobs:
+        n = len(pts[q])
+        if n < 20:  # the reference's pair_count exits below 20 query points (kdquery.c:176)
+            skipped.append(name)
+            continue
+        idx = np.sort(rs.choice(n, size=min(nq_max, n), replace=False))
+        f = w.catalogs[q][1]
+        samples.append((name, t, q, pts[q][idx], None if f is None else f[idx]))
+    times = [[] for _ in samples]
+    counts = [None] * len(samples)
     for it in range(warmup + steps):
-        for name, t, q, qf in jobs:
+        for j, (name, t, q, qp, qf) in enumerate(samples):
+            nthreads = max(1, min(cores, len(qp) // 20))  # pair_count exits above n/20
             t0 = time.perf_counter()
-            for r in radii:
-                R.pair_count(t, q, qf, N_FIELDS, r, nthreads)
+            out = [R.pair_count(rtrees[t], qp, qf, w.catalogs[q][2], r, nthreads)
+                   for r in w.radii]
             if it >= warmup:
-                per_type[name].append(time.perf_counter() - t0)
+                times[j].append(time.perf_counter() - t0)
+            counts[j] = np.stack(out)
+    nodes = {n: R.nodes(rtrees[n]) for n in used}
     visits = 0
-    nodes = {"DD": R.nodes(td), "DR": R.nodes(tr)}
-    nodes["RR"] = nodes["DR"]
-    for name, _, q, _ in jobs:
-        for r in radii:
-            visits += O.count_visits(nodes[name], q, r, nthreads=cores)
-    R.destroy(td)
-    R.destroy(tr)
-    tt = {k: float(np.median(v)) for k, v in per_type.items()}
-    t = sum(tt.values())
-    nq = {"DD": len(data), "DR": len(data), "RR": len(rand)}
-    full_s = sum(tt[k] * nq[k] / n_queries for k in tt)
-    return {"value": visits / t, "unit": UNIT, "cores": nthreads, "kind": "reference",
-            "sample": (f"{n_queries} seeded query points each for DD, DR and RR against the full "
-                       f"{len(data)}/{len(rand)}-point trees, {len(radii)} pair_count calls per "
-                       f"count type"),
-            "s_per_sample": t, "pairs_tested_per_sample": int(visits),
-            "full_result_s_extrapolated": full_s,
-            "note": "pairs tested on the CPU = reference traversal node visits"}
+    for name, t, q, qp, qf in samples:
+        for r in w.radii:
+            visits += O.count_visits(nodes[t], qp, r, nthreads=cores)
+    parity = None
+    if gpu is not None:
+        gt = {n: gpu.build_tree(w.catalogs[n][0], w.catalogs[n][1], w.catalogs[n][2])
+              for n in used}
+        parity = True
+        for (name, t, q, qp, qf), want in zip(samples, counts):
+            got = gpu.count_points(gt[t], qp, qf, w.catalogs[q][2], w.radii)
+            parity &= bool(np.array_equal(got, want))
+        for tr in gt.values():
+            gpu.destroy(tr)
+    for tr in rtrees.values():
+        R.destroy(tr)
+    tt = [float(np.median(v)) for v in times]
+    t_all = sum(tt)
+    full_s = sum(tj * len(pts[q]) / len(qp) for tj, (_, _, q, qp, _) in zip(tt, samples))
+    nsamp = sorted({len(s[3]) for s in samples})
+    res = {"value": visits / t_all, "unit": UNIT,
+           "cores": max(1, min(cores, nq_max // 20)), "kind": "reference",
+           "sample": (f"{'/'.join(map(str, nsamp))} seeded query points for each of the "
+                      f"{len(samples)} counts against the full trees, {len(w.radii)} "
+                      f"pair_count calls per count"),
+           "s_per_sample": t_all, "pairs_tested_per_sample": int(visits),
+           "full_result_s_extrapolated": full_s,
+           "note": "pairs tested on the CPU = reference traversal node visits"}
+    if skipped:
+        res["counts_skipped"] = skipped
+    if w.radec:
+        res["coordinates_bit_identical"] = coords_equal
+    if parity is not None:
+        res["gpu_counts_equal_reference_on_sample"] = parity
+    return res
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    data, fd, rand, fr, radii = make_workload(args.scale)
-    cb = cpu_baseline(data, fd, rand, fr, radii, n_queries=args.cpu_queries, steps=args.steps,
-                      warmup=args.warmup)
+    w = WORKLOADS[args.workload](args.scale)
+    cb = cpu_baseline(w, n_queries=args.cpu_queries, steps=args.steps, warmup=args.warmup)
     if cb.get("value") is None:
         print(json.dumps({"impl": "reference", "unavailable": cb.get("unavailable")}))
         return
+    sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
+    cfg = {"workload": w.description, "counts": len(w.jobs), "edges": len(w.radii)}
+    if len(sizes) <= 4:
+        cfg["catalogs"] = sizes
+    else:
+        cfg["catalogs"] = len(sizes)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": cb["s_per_sample"] * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic (seeded Neyman-Scott data and uniform randoms)",
-            "config": {"workload": WORKLOAD, "n_data": len(data), "n_rand": len(rand),
-                       "edges": len(radii), "fields": N_FIELDS},
+            "dtype": "f64", "data": w.data, "config": cfg,
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "full_result_s_extrapolated": cb["full_result_s_extrapolated"],
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -448,9 +666,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("mine", "reference"), default="mine")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="clustered3d")
     ap.add_argument("--scale", type=float, default=1.0, help="workload size factor (1 = full)")
-    ap.add_argument("--cpu-queries", type=int, default=4000,
-                    help="query points per count type in the CPU sample")
+    ap.add_argument("--cpu-queries", type=int, default=None,
+                    help="query points per count in the CPU sample (default per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mine":
