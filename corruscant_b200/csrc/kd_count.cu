@@ -48,6 +48,7 @@ constexpr int kQ = KD_QPL;              // query points per lane
 constexpr int kTileWarpsPerCta = 4;
 constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
+constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
 
 struct TreeSide {
     const double *x, *y, *z;
@@ -379,6 +380,26 @@ __device__ __forceinline__ void fp64_run(const double *__restrict__ tx,
     }
 }
 
+// Warp-cooperative exact recount of one query over a run: every lane takes
+// the points j = lane, lane + 32 (at most two, so each lane's per-edge count
+// is at most 2 and the warp sum at most 64: the four byte-packed counts add
+// without carries in one reduction).  Returns the packed counts in all lanes.
+__device__ __noinline__ unsigned exact_pass_warp(const double *__restrict__ tx,
+                                                 const double *__restrict__ ty,
+                                                 const double *__restrict__ tz, int rl,
+                                                 double qx, double qy, double qz,
+                                                 const double *R, int kn, int lane)
+{
+    unsigned part = 0;
+    for (int j = lane; j < rl; j += 32) {
+        const double d2 = d2_ref(__ldg(tx + j), __ldg(ty + j), __ldg(tz + j), qx, qy, qz);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (k < kn) part += (unsigned)(d2 < R[k]) << (8 * k);
+    }
+    return __reduce_add_sync(0xffffffffu, part);
+}
+
 // Exact recount of one query over a run (global FP64 coordinates), for band
 // rechecks and edges FP32 cannot represent; counts packed one per byte.  Out
 // of line so the FP32 loop stays small.
@@ -701,7 +722,30 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     }
                     redo = 0;
                 }
-                // exact FP64 recount of the queries FP32 could not decide
+                // exact FP64 recount of the queries FP32 could not decide: a
+                // few of them (band pairs) by the whole warp, one after the
+                // other; many (edges FP32 cannot represent) lane by lane
+                const unsigned nre = __reduce_add_sync(0xffffffffu, (unsigned)__popc(redo));
+                if (nre <= kCoopMax) {
+                    for (unsigned it = 0; it < nre; it++) {
+                        const unsigned has = __ballot_sync(0xffffffffu, redo != 0);
+                        const int src = __ffs(has) - 1;
+                        const int pq = __shfl_sync(0xffffffffu, __ffs(redo) - 1, src);
+                        const int qi = qs + kQ * src + pq;
+                        const unsigned pk =
+                            exact_pass_warp(J.tx + rs, J.ty + rs, J.tz + rs, rl, J.Q.x[qi],
+                                            J.Q.y[qi], J.Q.z[qi], R + k0 + kb, kn, lane);
+                        if (lane == src) {
+#pragma unroll
+                            for (int p = 0; p < kQ; p++)
+                                if (p == pq) {
+#pragma unroll
+                                    for (int k = 0; k < 4; k++) cnt[p][k] = (pk >> (8 * k)) & 0xFF;
+                                }
+                            redo &= ~(1u << pq);
+                        }
+                    }
+                }
 #pragma unroll
                 for (int p = 0; p < kQ; p++)
                     if ((redo >> p) & 1) {
