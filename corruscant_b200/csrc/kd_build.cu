@@ -1236,7 +1236,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     ro.tf = split ? keep.alloc<int>(n) : ro.qf;
     k_raw_scatter<<<grid_for(n), TPB, 0, s>>>(n, p3, cls, u.uhead, cpos, rstart, xyz, fin,
                                               u.ufield, ro, split);
-    int *leaf_r = pool.alloc<int>(nleaves + 1);
+    int *leaf_r = keep.alloc<int>(nleaves + 1);
     k_leaf_rstart<<<blocks_for(nleaves + 1, TPB), TPB, 0, s>>>(nleaves, ustart, rstart, leaf_r);
     KD_LAUNCH_CHECK("layout kernels");
 
@@ -1349,6 +1349,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     cat->d_ntf = keep.keep(sm.tf);
     cat->d_nqf = keep.keep(sm.qf);
     cat->d_leaf_run = keep.keep(leaf_run);
+    cat->d_leaf_pos = keep.keep(leaf_r);
     cat->nruns = nruns;
     cat->d_run_start = keep.keep(run_start);
     cat->d_run_len = keep.keep(run_len);
@@ -1436,7 +1437,8 @@ extern "C" void kdg_free(kd_catalog *cat)
     void *ptrs[] = {cat->d_nodes,    cat->d_inorder_rep, cat->d_x,       cat->d_y,
                     cat->d_z,        cat->d_qf,          cat->fields_split ? cat->d_tf : nullptr,
                     cat->d_box,      cat->d_ncount,      cat->d_ntf,     cat->d_nqf,
-                    cat->d_leaf_run, cat->d_run_start,   cat->d_run_len, cat->d_run_tf,
+                    cat->d_leaf_run, cat->d_leaf_pos,    cat->d_run_start, cat->d_run_len,
+                    cat->d_run_tf,
                     cat->d_run_leaf, cat->d_t4,          cat->d_leaf_c,
                     cat->d_blk_start, cat->d_blk_len,    cat->d_blk_qf,  cat->d_blk_box};
     for (void *p : ptrs)

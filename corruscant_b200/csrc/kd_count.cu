@@ -53,7 +53,7 @@ constexpr int kCoopMax = 32;            // rechecks of a run done by the whole w
 struct TreeSide {
     const double *x, *y, *z;
     const double *box;
-    const int *count, *tf, *leaf_run;
+    const int *count, *tf, *leaf_run, *leaf_pos;
     const int *run_start, *run_len, *run_tf;
     int D, nleaves;
 };
@@ -75,7 +75,13 @@ struct JobDesc {
     const double *leaf_c;        // 3 per leaf
     double hT;                   // largest leaf half-diagonal, with margin
     unsigned long long *H;       // (ne + 1) x Fqe x Fte bin histogram
+    // Symmetric job (tree and query are one catalog whose points all have own
+    // field == tree field): a block counts only tree points at or after its
+    // own first point; points inside the block as ordered pairs into H, points
+    // after it once into H2, and the host adds H2 and its field transpose.
+    unsigned long long *H2;
     int Fqe, Fte;
+    int sym, pad_;
 };
 static_assert(sizeof(JobDesc) % 8 == 0, "JobDesc is copied in 8-byte words");
 
@@ -155,9 +161,11 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
     const int b = g - jblk[j];
     const TreeSide T = jobs[j].T;
     const QuerySide Q = jobs[j].Q;
-    unsigned long long *const H = jobs[j].H;
+    unsigned long long *const H = jobs[j].H, *const H2 = jobs[j].H2;
     const int Fqe = jobs[j].Fqe, Fte = jobs[j].Fte;
+    const bool sym = jobs[j].sym != 0;
     const int alen = Q.blk_len[b], aqf = Q.blk_qf[b];
+    const int qb0 = Q.blk_start[b], qb1 = qb0 + alen;  // the block's raw positions
     double *bb = wb[w];
     if (lane < 6) bb[lane] = Q.blk_box[6 * (size_t)b + lane];
     int *st = stack[w];
@@ -179,22 +187,46 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
         sp -= nb;
         int act = 0, nr = 0, leaf = 0, elo = 0, ehi = 0;
         if (h) {
-            bin_range(bb, T.box + 6 * (size_t)h, rsq, ne, elo, ehi);
-            if (elo >= ne) {
+            // symmetric jobs: the node's raw positions [nlo, nhi) against the
+            // block's [qb0, qb1): before it -> nothing (the other side's block
+            // counts these pairs), after it -> once into H2, overlapping ->
+            // descend, runs cut at the block's ends
+            int nlo = 0, nhi = 0;
+            if (sym) {
+                const int sh = T.D - (31 - __clz(h));
+                nlo = T.leaf_pos[(h << sh) - T.nleaves];
+                nhi = T.leaf_pos[((h + 1) << sh) - T.nleaves];
+            }
+            const bool after = sym && nlo >= qb1;
+            if (sym && nhi <= qb0) {
                 act = 0;
-            } else if (elo == ehi && aqf >= 0 && T.tf[h] >= 0) {
-                if (FILL) {
-                    const unsigned long long c =
-                        (unsigned long long)alen * (unsigned long long)T.count[h];
-                    atomicAdd(&H[((size_t)elo * Fqe + aqf) * Fte + T.tf[h]], c);
-                    acc_pairs += c;
-                }
-            } else if (h >= T.nleaves) {
-                act = 2;
-                leaf = h - T.nleaves;
-                nr = T.leaf_run[leaf + 1] - T.leaf_run[leaf];
             } else {
-                act = 1;
+                bin_range(bb, T.box + 6 * (size_t)h, rsq, ne, elo, ehi);
+                const bool whole = !sym || after || (nlo >= qb0 && nhi <= qb1);
+                if (elo >= ne) {
+                    act = 0;
+                } else if (whole && elo == ehi && aqf >= 0 && T.tf[h] >= 0) {
+                    if (FILL) {
+                        const unsigned long long c =
+                            (unsigned long long)alen * (unsigned long long)T.count[h];
+                        atomicAdd(&(after ? H2 : H)[((size_t)elo * Fqe + aqf) * Fte + T.tf[h]], c);
+                        acc_pairs += c;
+                    }
+                } else if (h >= T.nleaves) {
+                    act = 2;
+                    leaf = h - T.nleaves;
+                    const int r0 = T.leaf_run[leaf], r1 = T.leaf_run[leaf + 1];
+                    if (!sym) {
+                        nr = r1 - r0;
+                    } else {
+                        for (int r = r0; r < r1; r++) {
+                            const int a = T.run_start[r], e = a + T.run_len[r];
+                            nr += (max(a, qb0) < min(e, qb1)) + (max(a, qb1) < e);
+                        }
+                    }
+                } else {
+                    act = 1;
+                }
             }
         }
         int ps = act == 1 ? 2 : 0;
@@ -220,14 +252,23 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
         const int etot = __shfl_sync(0xffffffffu, es, 31);
         if (FILL && act == 2) {
             const unsigned code = (unsigned)elo | ((unsigned)(ehi - elo) << 8);
-            const int r0 = T.leaf_run[leaf];
-            for (int k = 0; k < nr; k++) {
-                const long long idx = base + emitted + es - nr + k;
-                const int r = r0 + k;
-                o.rec[idx] = make_uint4((unsigned)T.run_start[r], (unsigned)leaf,
-                                        (unsigned)T.run_len[r] | ((unsigned)T.run_tf[r] << 8) |
-                                            (code << 16),
-                                        0u);
+            const int r0 = T.leaf_run[leaf], r1 = T.leaf_run[leaf + 1];
+            long long idx = base + emitted + es - nr;
+            // record: start, leaf, length | tree field << 8 | edges << 16, and
+            // w = 1 for the once-counted (H2) part of a symmetric job
+            auto put = [&](int a, int len, int tf, unsigned once) {
+                o.rec[idx++] = make_uint4((unsigned)a, (unsigned)leaf,
+                                          (unsigned)len | ((unsigned)tf << 8) | (code << 16), once);
+            };
+            for (int r = r0; r < r1; r++) {
+                const int a = T.run_start[r], e = a + T.run_len[r];
+                if (!sym) {
+                    put(a, e - a, T.run_tf[r], 0u);
+                } else {
+                    const int ia = max(a, qb0), ib = min(e, qb1), aa = max(a, qb1);
+                    if (ia < ib) put(ia, ib - ia, T.run_tf[r], 0u);
+                    if (aa < e) put(aa, e - aa, T.run_tf[r], 1u);
+                }
             }
         }
         emitted += etot;
@@ -555,7 +596,10 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
         int since = 0;
         int tlo = ne, thi = -1;  // bins written since the last flush
 
-        auto flush = [&](int tf) {
+        // flush key: tree field | 256 for the once-counted part of a symmetric job
+        auto flush = [&](int key) {
+            const int tf = key & 0xFF;
+            unsigned long long *const Hd = (key >> 8) ? J.H2 : J.H;
             int qf[kQ];
 #pragma unroll
             for (int p = 0; p < kQ; p++) qf[p] = qfield(p);
@@ -577,14 +621,14 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         for (int p = 0; p < kQ; p++) sum += qf[p] == uf ? v[p] : 0;
                         for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
                         if (lane == 0 && sum)
-                            atomicAdd(&J.H[((size_t)e * J.Fqe + uf) * J.Fte + tf],
+                            atomicAdd(&Hd[((size_t)e * J.Fqe + uf) * J.Fte + tf],
                                       (unsigned long long)sum);
                     }
                 } else {
 #pragma unroll
                     for (int p = 0; p < kQ; p++)
                         if (((vmask >> p) & 1) && v[p])
-                            atomicAdd(&J.H[((size_t)e * J.Fqe + qf[p]) * J.Fte + tf],
+                            atomicAdd(&Hd[((size_t)e * J.Fqe + qf[p]) * J.Fte + tf],
                                       (unsigned long long)v[p]);
                 }
             }
@@ -662,9 +706,10 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             __syncwarp();
             if (i + 1 < ecnt) issue(i + 1);
 
-            if (tf != cur_tf || since + rl > 0xFFFF) {
+            const int key = tf | (int)(rec.w << 8);
+            if (key != cur_tf || since + rl > 0xFFFF) {
                 if (cur_tf >= 0) flush(cur_tf);
-                cur_tf = tf;
+                cur_tf = key;
                 since = 0;
             }
             since += rl;
@@ -832,6 +877,7 @@ static JobDesc job_desc(const kd_catalog *tc, const kd_catalog *qc, unsigned lon
     d.T.count = tc->d_ncount;
     d.T.tf = tc->d_ntf;
     d.T.leaf_run = tc->d_leaf_run;
+    d.T.leaf_pos = tc->d_leaf_pos;
     d.T.run_start = tc->d_run_start;
     d.T.run_len = tc->d_run_len;
     d.T.run_tf = tc->d_run_tf;
@@ -852,9 +898,21 @@ static JobDesc job_desc(const kd_catalog *tc, const kd_catalog *qc, unsigned lon
     d.leaf_c = tc->d_leaf_c;
     d.hT = tc->leaf_hdiag * (1.0 + 1e-12);
     d.H = H;
+    d.H2 = nullptr;
     d.Fqe = qc->max_qf + 1;
     d.Fte = tc->max_tf + 1;
+    d.sym = 0;
     return d;
+}
+
+// An autocorrelation count (one catalog on both sides) whose points all keep
+// their own field on the tree side can count each unordered pair once: the
+// distance of (q, t) and of (t, q) is the same double (t - q and q - t differ
+// only in sign, so every square, product and FMA is identical), and the pair's
+// second orientation lands in the transposed field cell.
+static bool symmetric_job(const kd_catalog *tc, const kd_catalog *qc)
+{
+    return tc == qc && !tc->fields_split && tc->max_qf == tc->max_tf;
 }
 
 static size_t hist_size(const kd_catalog *tc, const kd_catalog *qc, int ne)
@@ -883,15 +941,24 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
     // job table, histogram offsets, global block numbering
     std::vector<size_t> hoff(njobs + 1, 0);
     std::vector<int> hblk(njobs + 1, 0);
+    std::vector<char> sym(njobs);
     for (int j = 0; j < njobs; j++) {
-        hoff[j + 1] = hoff[j] + hist_size(tcs[j], qcs[j], ne);
+        sym[j] = symmetric_job(tcs[j], qcs[j]);
+        // a symmetric job has its once-counted histogram H2 right after H
+        hoff[j + 1] = hoff[j] + (sym[j] ? 2 : 1) * hist_size(tcs[j], qcs[j], ne);
         if ((long long)hblk[j] + qcs[j]->nblocks > INT_MAX) raise(KD_EINVAL, "too many query blocks in one count");
         hblk[j + 1] = hblk[j] + qcs[j]->nblocks;
     }
     const size_t hsz = hoff[njobs];
     unsigned long long *H = pool.alloc<unsigned long long>(hsz);
     std::vector<JobDesc> hj(njobs);
-    for (int j = 0; j < njobs; j++) hj[j] = job_desc(tcs[j], qcs[j], H + hoff[j]);
+    for (int j = 0; j < njobs; j++) {
+        hj[j] = job_desc(tcs[j], qcs[j], H + hoff[j]);
+        if (sym[j]) {
+            hj[j].sym = 1;
+            hj[j].H2 = H + hoff[j] + hist_size(tcs[j], qcs[j], ne);
+        }
+    }
     JobDesc *jobs = pool.alloc<JobDesc>(njobs);
     int *jblk = pool.alloc<int>(njobs + 1);
     unsigned long long *dstats = pool.alloc<unsigned long long>(8);
@@ -1013,8 +1080,21 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
     check(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
     st.sync();
     if (herr) raise(herr, "node-pair traversal exceeded its stack");
-    for (int j = 0; j < njobs; j++)
-        for (size_t i = hoff[j]; i < hoff[j + 1]; i++) hists[j][i - hoff[j]] = (long long)hh[i];
+    for (int j = 0; j < njobs; j++) {
+        const size_t n1 = hist_size(tcs[j], qcs[j], ne);
+        const unsigned long long *h1 = hh.data() + hoff[j];
+        for (size_t i = 0; i < n1; i++) hists[j][i] = (long long)h1[i];
+        if (sym[j]) {  // both orientations of the once-counted pairs
+            const unsigned long long *h2 = h1 + n1;
+            const size_t F = (size_t)hj[j].Fqe;
+            for (int e = 0; e <= ne; e++)
+                for (size_t a = 0; a < F; a++)
+                    for (size_t c = 0; c < F; c++)
+                        hists[j][((size_t)e * F + a) * F + c] +=
+                            (long long)(h2[((size_t)e * F + a) * F + c] +
+                                        h2[((size_t)e * F + c) * F + a]);
+        }
+    }
     if (stats) {
         stats->pairs_tested = (long long)hs[0];
         stats->pairs_rechecked = (long long)hs[1];

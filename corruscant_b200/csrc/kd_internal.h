@@ -78,6 +78,7 @@ typedef struct kd_catalog {
     int *d_ntf;       /* single tree field of the node, -1 when mixed */
     int *d_nqf;       /* single own field of the node, -1 when mixed */
     int *d_leaf_run;  /* nleaves+1: first run of each leaf */
+    int *d_leaf_pos;  /* nleaves+1: first raw position (counting order) of each leaf */
 
     int nruns;
     int *d_run_start, *d_run_len, *d_run_tf, *d_run_leaf;
