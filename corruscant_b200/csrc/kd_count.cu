@@ -335,7 +335,7 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
                                              const float2 (&qy)[kQ / 2],
                                              const float2 (&qz)[kQ / 2],
                                              const float (&a)[kQ][kPass32],
-                                             const float (&nsl)[kPass32], int (&cnt)[kQ][4])
+                                             const float (&nsl)[kPass32], unsigned (&pc)[kQ / 2][4])
 {
     float2 acc[kQ / 2][K], acc2[kQ / 2];
 #pragma unroll
@@ -360,25 +360,32 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
         }
     };
     int j = 0;
-    for (; j + 2 <= rl; j += 2) {
+    for (; j + 4 <= rl; j += 4) {
         const float4 t0 = ts[2 * j], t1 = ts[2 * j + 1], t2 = ts[2 * j + 2], t3 = ts[2 * j + 3];
+        const float4 t4 = ts[2 * j + 4], t5 = ts[2 * j + 5], t6 = ts[2 * j + 6], t7 = ts[2 * j + 7];
         point(t0, t1);
         point(t2, t3);
+        point(t4, t5);
+        point(t6, t7);
     }
-    if (j < rl) point(ts[2 * j], ts[2 * j + 1]);
+    for (; j < rl; j++) point(ts[2 * j], ts[2 * j + 1]);
+    // Counts without the conversion unit: v + 1.5 * 2^23 lands on the integer
+    // grid of that binade, so the low 16 bits of its pattern are round(v)
+    // (0 <= v <= 256; the bias 0x4B400000 has zero low half).  The two
+    // queries of a pair are packed as (query 2h) | (query 2h + 1) << 16.
+    const float2 bias = make_float2(12582912.0f, 12582912.0f);
     unsigned band = 0;
 #pragma unroll
-    for (int p = 0; p < kQ; p++) {
-        float tot = 0.0f;
+    for (int h = 0; h < kQ / 2; h++) {
+        float2 tot = make_float2(0.0f, 0.0f);
 #pragma unroll
         for (int k = 0; k < K; k++) {
-            const float v = p & 1 ? acc[p >> 1][k].y : acc[p >> 1][k].x;
-            tot += v;
-            // nearest integer of 0 <= v <= 256 without the conversion unit:
-            // v + 1.5 * 2^23 lands on the integer grid of that binade
-            cnt[p][k] = __float_as_int(v + 12582912.0f) - 0x4B400000;
+            tot = __fadd2_rn(tot, acc[h][k]);
+            const float2 b = __fadd2_rn(acc[h][k], bias);
+            pc[h][k] = __byte_perm(__float_as_uint(b.x), __float_as_uint(b.y), 0x5410);
         }
-        if (tot != (p & 1 ? acc2[p >> 1].y : acc2[p >> 1].x)) band |= 1u << p;
+        if (tot.x != acc2[h].x) band |= 1u << (2 * h);
+        if (tot.y != acc2[h].y) band |= 2u << (2 * h);
     }
     return band;
 }
@@ -547,11 +554,12 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             qy2[h] = make_float2(qy[2 * h], qy[2 * h + 1]);
             qz2[h] = make_float2(qz[2 * h], qz[2 * h + 1]);
         }
-        // packed increment of the two queries of word h (invalid ones add 0)
-        auto pk = [&](int h, int d0, int d1) {
-            return (((vmask >> (2 * h)) & 1) ? (unsigned)d0 : 0u) |
-                   ((((vmask >> (2 * h + 1)) & 1) ? (unsigned)d1 : 0u) << 16);
-        };
+        // half-word masks of the valid queries of each pair (invalid add 0)
+        unsigned vm[kQ / 2];
+#pragma unroll
+        for (int h = 0; h < kQ / 2; h++)
+            vm[h] = (((vmask >> (2 * h)) & 1) ? 0xFFFFu : 0u) |
+                    (((vmask >> (2 * h + 1)) & 1) ? 0xFFFF0000u : 0u);
         auto qfield = [&](int p) { return ((vmask >> p) & 1) ? J.Q.qf[qbase + p] : -1; };
         // the distinct own fields of the block (up to kMaxDistinctQf are
         // reduced per warp at a flush; beyond that, per-query atomics)
@@ -717,19 +725,25 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             thi = max(thi, k0 + K);
             if (K == 0) {
 #pragma unroll
-                for (int h = 0; h < kQ / 2; h++) P[(k0 * (kQ / 2) + h) * 32 + lane] += pk(h, rl, rl);
+                for (int h = 0; h < kQ / 2; h++)
+                    P[(k0 * (kQ / 2) + h) * 32 + lane] += (((unsigned)rl | ((unsigned)rl << 16)) & vm[h]);
                 __syncwarp();
                 continue;
             }
             wtiles++;
             const bool fp32 = MODE == KD_MODE_MIXED && isfinite(R[k0 + K - 1]);
-            int prev[kQ];
+            // packed cumulative count of the previous edge, per query pair
+            unsigned prev[kQ / 2];
 #pragma unroll
-            for (int p = 0; p < kQ; p++) prev[p] = 0;
+            for (int h = 0; h < kQ / 2; h++) prev[h] = 0;
             const int pw = MODE == KD_MODE_MIXED && fp32 ? kPass32 : 4;
             for (int kb = 0; kb < K; kb += pw) {
                 const int kn = min(pw, K - kb);
-                int cnt[kQ][4];
+                unsigned pc[kQ / 2][4];
+#pragma unroll
+                for (int h = 0; h < kQ / 2; h++)
+#pragma unroll
+                    for (int k = 0; k < 4; k++) pc[h][k] = 0;
                 unsigned redo = vmask;
                 if (fp32) {
                     float a[kQ][kPass32], sl[kPass32];
@@ -742,10 +756,10 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     }
                     unsigned band;
                     switch (kn) {
-                    case 1: band = fp32_run<1>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
-                    case 2: band = fp32_run<2>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
-                    case 3: band = fp32_run<3>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
-                    default: band = fp32_run<4>(ws->stage, rl, qx2, qy2, qz2, a, sl, cnt); break;
+                    case 1: band = fp32_run<1>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    case 2: band = fp32_run<2>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    case 3: band = fp32_run<3>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    default: band = fp32_run<4>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
                     }
                     redo = band & vmask;
                     rechecked += (unsigned long long)__popc(redo) * rl;
@@ -759,12 +773,18 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         qzd[p] = v ? J.Q.z[qbase + p] : oz;
                     }
                     const double *s64 = ws->stage64;
+                    int cnt[kQ][4];
                     switch (kn) {
                     case 1: fp64_run<1>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
                     case 2: fp64_run<2>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
                     case 3: fp64_run<3>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
                     default: fp64_run<4>(s64, s64 + KD_RUN_MAX, s64 + 2 * KD_RUN_MAX, rl, qxd, qyd, qzd, R + k0 + kb, cnt); break;
                     }
+#pragma unroll
+                    for (int h = 0; h < kQ / 2; h++)
+#pragma unroll
+                        for (int k = 0; k < 4; k++)
+                            pc[h][k] = (unsigned)cnt[2 * h][k] | ((unsigned)cnt[2 * h + 1][k] << 16);
                     redo = 0;
                 }
                 // exact FP64 recount of the queries FP32 could not decide: a
@@ -781,12 +801,17 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                             exact_pass_warp(J.tx + rs, J.ty + rs, J.tz + rs, rl, J.Q.x[qi],
                                             J.Q.y[qi], J.Q.z[qi], R + k0 + kb, kn, lane);
                         if (lane == src) {
+                            // replace query pq's half-word (selects, no indexing)
 #pragma unroll
-                            for (int p = 0; p < kQ; p++)
-                                if (p == pq) {
+                            for (int h = 0; h < kQ / 2; h++) {
+                                const bool lo = pq == 2 * h, hi = pq == 2 * h + 1;
 #pragma unroll
-                                    for (int k = 0; k < 4; k++) cnt[p][k] = (pk >> (8 * k)) & 0xFF;
+                                for (int k = 0; k < 4; k++) {
+                                    const unsigned v = (pk >> (8 * k)) & 0xFFu;
+                                    pc[h][k] = lo ? ((pc[h][k] & 0xFFFF0000u) | v)
+                                                  : hi ? ((pc[h][k] & 0xFFFFu) | (v << 16)) : pc[h][k];
                                 }
+                            }
                             redo &= ~(1u << pq);
                         }
                     }
@@ -797,23 +822,27 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         const unsigned pk =
                             exact_pass(J.tx + rs, J.ty + rs, J.tz + rs, rl, J.Q.x[qbase + p],
                                        J.Q.y[qbase + p], J.Q.z[qbase + p], R + k0 + kb, kn);
+                        const int sh = 16 * (p & 1);
 #pragma unroll
-                        for (int k = 0; k < 4; k++) cnt[p][k] = (pk >> (8 * k)) & 0xFF;
+                        for (int k = 0; k < 4; k++)
+                            pc[p >> 1][k] = (pc[p >> 1][k] & ~(0xFFFFu << sh)) |
+                                            (((pk >> (8 * k)) & 0xFFu) << sh);
                     }
+                // bin increments: packed cumulative counts minus the previous
+                // edge's (no borrow between the halves: counts grow with k)
 #pragma unroll
                 for (int h = 0; h < kQ / 2; h++)
 #pragma unroll
                     for (int k = 0; k < 4; k++)
                         if (k < kn) {
-                            P[((k0 + kb + k) * (kQ / 2) + h) * 32 + lane] +=
-                                pk(h, cnt[2 * h][k] - prev[2 * h], cnt[2 * h + 1][k] - prev[2 * h + 1]);
-                            prev[2 * h] = cnt[2 * h][k];
-                            prev[2 * h + 1] = cnt[2 * h + 1][k];
+                            P[((k0 + kb + k) * (kQ / 2) + h) * 32 + lane] += (pc[h][k] - prev[h]) & vm[h];
+                            prev[h] = pc[h][k];
                         }
             }
+            const unsigned rl2 = (unsigned)rl | ((unsigned)rl << 16);
 #pragma unroll
             for (int h = 0; h < kQ / 2; h++)
-                P[((k0 + K) * (kQ / 2) + h) * 32 + lane] += pk(h, rl - prev[2 * h], rl - prev[2 * h + 1]);
+                P[((k0 + K) * (kQ / 2) + h) * 32 + lane] += (rl2 - prev[h]) & vm[h];
             const unsigned long long tp = (unsigned long long)nvalid * rl;
             pairs += tp;
             kpairs += tp * K;
