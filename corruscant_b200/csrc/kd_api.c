@@ -16,6 +16,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 
 #include "kd_internal.h"
 
@@ -98,8 +99,22 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
         free(h);
         return t;
     }
-    /* calloc: empty heap slots stay zero, as in kdbuild.c:516 */
-    h->nodes = (node_t *)calloc((size_t)h->cat.memsize, sizeof(node_t));
+    /* every byte is written by the copy: empty heap slots come zeroed from
+     * the device (as calloc leaves them in kdbuild.c:516) */
+    {
+        const size_t nb = (size_t)h->cat.memsize * sizeof(node_t);
+        void *mem = NULL;
+        if (nb >= ((size_t)64 << 20)) {
+            /* large node arrays (1.3 GB at 20M points) in 2 MB pages where
+             * the kernel offers them: the copy below then takes a few hundred
+             * page faults instead of hundreds of thousands */
+            if (posix_memalign(&mem, (size_t)2 << 20, nb) != 0) mem = NULL;
+            if (mem) madvise(mem, nb, MADV_HUGEPAGE);
+        } else {
+            mem = malloc(nb);
+        }
+        h->nodes = (node_t *)mem;
+    }
     if (!h->nodes || kdg_copy_nodes(&h->cat, h->nodes) != KD_OK) {
         if (!h->nodes) kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
         free(h->nodes);

@@ -36,6 +36,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <thread>
+#include <vector>
 
 #include "kd_cuda_util.cuh"
 
@@ -1396,6 +1399,71 @@ struct OnDevice {
     ~OnDevice() { cudaSetDevice(prev); }
 };
 
+namespace kd {
+
+// Device -> pageable host copy of a large array (the node array returned by
+// tree_construct, 1.3 GB at 20M points).  A plain cudaMemcpy into freshly
+// allocated pageable memory runs at the speed of the page faults of its one
+// copying thread; here the data goes through two pinned staging chunks (the
+// next chunk's DMA overlaps the current one's host copy) and each chunk is
+// copied into the destination by several threads, which take the destination's
+// first-touch page faults in parallel.
+static void copy_to_pageable(void *dst, const void *src, size_t bytes)
+{
+    const size_t chunk = size_t(32) << 20;
+    if (bytes <= chunk) {
+        check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "D2H");
+        return;
+    }
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    Stream st;
+    void *pin[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    struct Release {
+        void **pin;
+        cudaEvent_t *ev;
+        ~Release()
+        {
+            for (int i = 0; i < 2; i++) {
+                if (pin[i]) cudaFreeHost(pin[i]);
+                if (ev[i]) cudaEventDestroy(ev[i]);
+            }
+        }
+    } rel{pin, done};
+    for (int i = 0; i < 2; i++) {
+        check(cudaMallocHost(&pin[i], chunk), "cudaMallocHost");
+        check(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    const size_t nch = (bytes + chunk - 1) / chunk;
+    auto issue = [&](size_t c) {
+        const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+        check(cudaMemcpyAsync(pin[c & 1], (const char *)src + off, len, cudaMemcpyDeviceToHost, st.s),
+              "D2H");
+        check(cudaEventRecord(done[c & 1], st.s), "event");
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthr = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+    issue(0);
+    for (size_t c = 0; c < nch; c++) {
+        check(cudaEventSynchronize(done[c & 1]), "D2H wait");
+        if (c + 1 < nch) issue(c + 1);  // into the other buffer, already drained
+        const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+        const char *from = (const char *)pin[c & 1];
+        char *to = (char *)dst + off;
+        std::vector<std::thread> th;
+        for (int t = 1; t < nthr; t++) {
+            const size_t a = len * t / nthr, b = len * (t + 1) / nthr;
+            th.emplace_back([=] { std::memcpy(to + a, from + a, b - a); });
+        }
+        std::memcpy(to, from, len / nthr);
+        for (auto &x : th) x.join();
+    }
+    (void)dev;
+}
+
+}  // namespace kd
+
 extern "C" int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
 {
     OnDevice on(cat->device);
@@ -1403,11 +1471,11 @@ extern "C" int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
         kd_set_error(KD_EINVAL, "node array no longer held on the device");
         return KD_EINVAL;
     }
-    cudaError_t e = cudaMemcpy(h_nodes, cat->d_nodes, sizeof(kd::NodeRec) * (size_t)cat->memsize,
-                               cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) {
-        kd_set_error(KD_ECUDA, "node copy: %s", cudaGetErrorString(e));
-        return KD_ECUDA;
+    try {
+        kd::copy_to_pageable(h_nodes, cat->d_nodes, sizeof(kd::NodeRec) * (size_t)cat->memsize);
+    } catch (const kd::Error &e) {
+        kd_set_error(e.code, "node copy: %s", e.msg);
+        return e.code;
     }
     return KD_OK;
 }
