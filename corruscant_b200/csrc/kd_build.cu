@@ -37,6 +37,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -53,11 +54,13 @@ struct alignas(8) NodeRec {
 };
 static_assert(sizeof(NodeRec) == 40, "node_t is 40 bytes");
 
-// Segments up to this size get the exact sequential variance directly.
-constexpr int kSmallSeg = 4096;
-// Positions per block in the parallel variance kernels (< kSmallSeg so a
+// Segments up to this size get the exact sequential variance directly;
+// larger ones first try the parallel sums with a rigorous interval (one
+// thread walking thousands of gathered points is slow: ~1 us per point).
+constexpr int kSmallSeg = 256;
+// Positions per block in the parallel variance kernels (<= kSmallSeg + 1 so a
 // block touches at most two segments).
-constexpr int kVarChunk = 2048;
+constexpr int kVarChunk = 256;
 
 void init_device()
 {
@@ -1415,26 +1418,30 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
         check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "D2H");
         return;
     }
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
+    // two pinned staging chunks kept for the life of the process (allocating
+    // pinned memory per call costs more than the copy); calls that find them
+    // in use by another thread fall back to a plain copy
+    static std::mutex mu;
+    static void *pin[2] = {nullptr, nullptr};
+    std::unique_lock<std::mutex> lock(mu, std::try_to_lock);
+    if (!lock.owns_lock()) {
+        check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "D2H");
+        return;
+    }
+    for (int i = 0; i < 2; i++)
+        if (!pin[i]) check(cudaHostAlloc(&pin[i], chunk, cudaHostAllocPortable), "cudaHostAlloc");
     Stream st;
-    void *pin[2] = {nullptr, nullptr};
     cudaEvent_t done[2] = {nullptr, nullptr};
     struct Release {
-        void **pin;
         cudaEvent_t *ev;
         ~Release()
         {
-            for (int i = 0; i < 2; i++) {
-                if (pin[i]) cudaFreeHost(pin[i]);
+            for (int i = 0; i < 2; i++)
                 if (ev[i]) cudaEventDestroy(ev[i]);
-            }
         }
-    } rel{pin, done};
-    for (int i = 0; i < 2; i++) {
-        check(cudaMallocHost(&pin[i], chunk), "cudaMallocHost");
+    } rel{done};
+    for (int i = 0; i < 2; i++)
         check(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
-    }
     const size_t nch = (bytes + chunk - 1) / chunk;
     auto issue = [&](size_t c) {
         const size_t off = c * chunk, len = std::min(chunk, bytes - off);
@@ -1459,7 +1466,6 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
         std::memcpy(to, from, len / nthr);
         for (auto &x : th) x.join();
     }
-    (void)dev;
 }
 
 }  // namespace kd
