@@ -113,6 +113,24 @@ def main():
     counts["layout_q2_t3/qfields"] = qf
     counts["layout_q2_t3/counts"] = np.stack([R.pair_count(t, q, qf, 2, r, 1) for r in RADII])
     R.destroy(t)
+    # field ids beyond 255: the reference's node keeps only the low 8 bits
+    # (kdtree.h: field:8) while the query side keeps the full id
+    rs2 = np.random.RandomState(300)
+    p = rs2.rand(600, 3)
+    f = rs2.randint(0, 300, 600).astype(np.int32)
+    t = R.build(p, f, 300)
+    trees["fields300/points"] = p
+    trees["fields300/fields"] = f
+    trees["fields300/num_fields"] = np.array(300)
+    trees["fields300/size"] = np.array(t.size)
+    for k, v in R.nodes(t).items():
+        trees[f"fields300/node_{k}"] = v
+    q = np.concatenate([p, rs2.rand(64, 3)])
+    qf = np.concatenate([f, rs2.randint(0, 300, 64).astype(np.int32)])
+    counts["fields300/queries"] = q
+    counts["fields300/qfields"] = qf
+    counts["fields300/counts"] = np.stack([R.pair_count(t, q, qf, 300, r, 1) for r in RADII])
+    R.destroy(t)
     counts["radii"] = RADII
     np.savez_compressed(os.path.join(HERE, "trees.npz"), **trees)
     np.savez_compressed(os.path.join(HERE, "counts.npz"), **counts)
