@@ -109,6 +109,8 @@ def kdlib():
                                       POINTER(CountStats)]
         L.kd_tree_permutation.restype = c_int
         L.kd_tree_permutation.argtypes = [KdTree, POINTER(c_int)]
+        L.kd_set_precision.restype = c_int
+        L.kd_set_precision.argtypes = [c_int]
         L.kd_set_device.restype = c_int
         L.kd_set_device.argtypes = [c_int]
         L.kd_tree_input_size.restype = c_int
@@ -250,6 +252,12 @@ def permutation(tree):
     if kdlib().kd_tree_permutation(tree, iptr(perm)) != 0:
         raise_last()
     return perm
+
+
+def set_precision(mode):
+    """Mode of pair_count on this thread (kd_set_precision)."""
+    if kdlib().kd_set_precision(c_int(mode)) != 0:
+        raise_last()
 
 
 def set_device(device):

@@ -514,6 +514,20 @@ int kd_count_radii_static(kdtree_t tree, kdtree_t query, const double *radii, in
                             edge_of, nradii, mode, out);
 }
 
+/* mode used by pair_count on the calling thread (kd_set_precision) */
+static __thread int g_pair_mode = KD_MODE_MIXED;
+
+int kd_set_precision(int mode)
+{
+    clear_error();
+    if (mode != KD_MODE_MIXED && mode != KD_MODE_FP64) {
+        kd_set_error(KD_EINVAL, "kd_set_precision: unknown mode %d", mode);
+        return KD_EINVAL;
+    }
+    g_pair_mode = mode;
+    return KD_OK;
+}
+
 long long *pair_count(kdtree_t tree, double *data, int *fields, int length, int num_fields,
                       double r, int num_threads)
 {
@@ -525,7 +539,7 @@ long long *pair_count(kdtree_t tree, double *data, int *fields, int length, int 
         kd_set_error(KD_ENOMEM, "out of host memory");
         return NULL;
     }
-    if (kd_count_points(tree, data, fields, length, num_fields, &r, 1, KD_MODE_MIXED, out, NULL) !=
+    if (kd_count_points(tree, data, fields, length, num_fields, &r, 1, g_pair_mode, out, NULL) !=
         KD_OK) {
         free(out);
         return NULL;

@@ -112,6 +112,13 @@ typedef struct kd_count_stats {
  * the message into buf (may be NULL). */
 int kd_last_error(char *buf, int len);
 
+/* Selects how pair_count counts on the calling thread: KD_MODE_MIXED (FP32
+ * with exact FP64 rechecks near every edge, the default) or KD_MODE_FP64
+ * (every distance in FP64).  Both give the reference's counts exactly.  The
+ * reference's pair_count (src/kdquery.c:165) has no precision argument; this
+ * keeps its signature unchanged.  Returns 0 or KD_EINVAL. */
+int kd_set_precision(int mode);
+
 /* Frees an array returned by pair_count. */
 void kd_free_counts(long long *counts);
 

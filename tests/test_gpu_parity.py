@@ -63,9 +63,12 @@ def test_pair_count_matches_reference_goldens(golden):
             fq = int(ts["num_fields"])
         qf = none_if_empty(s["qfields"])
         try:
-            for k, r in enumerate(radii):
-                got = N.pair_count(t, s["queries"], qf, fq, r)
-                assert np.array_equal(got, s["counts"][k]), (name, r)
+            for mode in MODES:  # the reference entry point in both precisions
+                N.set_precision(mode)
+                for k, r in enumerate(radii):
+                    got = N.pair_count(t, s["queries"], qf, fq, r)
+                    assert np.array_equal(got, s["counts"][k]), (name, r, mode)
+            N.set_precision(N.KD_MODE_MIXED)
             for mode in MODES:
                 got = N.count_points(t, s["queries"], qf, fq, radii, mode=mode)
                 assert np.array_equal(got, s["counts"]), (name, mode)

@@ -120,3 +120,13 @@ def test_coordinates_bit_identical_to_reference(golden):
 def test_chord_edges_are_the_reference_expression():
     deg = np.logspace(-3, np.log10(2.0), 16)
     _assert_bits(twopoint.angular.chord(deg), 2. * np.sin(deg * (np.pi / 180.) / 2.))
+
+
+def test_set_precision_validates_mode():
+    """kd_set_precision is host-only state for pair_count; unknown modes are
+    refused with an error instead of being stored."""
+    from corruscant_b200 import _native as N
+    N.set_precision(N.KD_MODE_FP64)
+    N.set_precision(N.KD_MODE_MIXED)
+    with pytest.raises(N.NativeError):
+        N.set_precision(7)
