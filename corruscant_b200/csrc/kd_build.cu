@@ -35,6 +35,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <exception>
+#include <new>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -1387,6 +1389,12 @@ extern "C" int kdg_build(const double *h_xyz, const int *h_fields, int n, int nu
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);
         return e.code;
+    } catch (const std::bad_alloc &) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return KD_ENOMEM;
+    } catch (const std::exception &e) {
+        kd_set_error(KD_EINTERNAL, "host error: %s", e.what());
+        return KD_EINTERNAL;
     }
 }
 
@@ -1459,11 +1467,16 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
         const char *from = (const char *)pin[c & 1];
         char *to = (char *)dst + off;
         std::vector<std::thread> th;
-        for (int t = 1; t < nthr; t++) {
-            const size_t a = len * t / nthr, b = len * (t + 1) / nthr;
-            th.emplace_back([=] { std::memcpy(to + a, from + a, b - a); });
+        bool spawned = true;
+        try {
+            for (int t = 1; t < nthr; t++) {
+                const size_t a = len * t / nthr, b = len * (t + 1) / nthr;
+                th.emplace_back([=] { std::memcpy(to + a, from + a, b - a); });
+            }
+        } catch (const std::exception &) {  // no more threads: this one copies the chunk
+            spawned = false;
         }
-        std::memcpy(to, from, len / nthr);
+        std::memcpy(to, from, spawned ? len / nthr : len);
         for (auto &x : th) x.join();
     }
 }
@@ -1482,6 +1495,12 @@ extern "C" int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "node copy: %s", e.msg);
         return e.code;
+    } catch (const std::bad_alloc &) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return KD_ENOMEM;
+    } catch (const std::exception &e) {
+        kd_set_error(KD_EINTERNAL, "host error: %s", e.what());
+        return KD_EINTERNAL;
     }
     return KD_OK;
 }

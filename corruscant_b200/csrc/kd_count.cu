@@ -32,6 +32,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <exception>
+#include <new>
 #include <climits>
 #include <cstring>
 #include <cmath>
@@ -1365,6 +1367,12 @@ extern "C" int kdg_count_static(const kd_catalog *tree, int Ft, const kd_catalog
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);
         return e.code;
+    } catch (const std::bad_alloc &) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return KD_ENOMEM;
+    } catch (const std::exception &e) {
+        kd_set_error(KD_EINTERNAL, "host error: %s", e.what());
+        return KD_EINTERNAL;
     }
 }
 
@@ -1406,6 +1414,12 @@ extern "C" int kdg_count_batch(const kd_catalog *const *trees, const kd_catalog 
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);
         return e.code;
+    } catch (const std::bad_alloc &) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return KD_ENOMEM;
+    } catch (const std::exception &e) {
+        kd_set_error(KD_EINTERNAL, "host error: %s", e.what());
+        return KD_EINTERNAL;
     }
 }
 
