@@ -325,10 +325,15 @@ def sm_count(device):
         return None
 
 
-def shard_range(n, shard, nshards):
-    """[lo, hi) of shard `shard` of n items split evenly over nshards, the
-    split kd_count_radii_shard and kd_count_batch_shard apply to query blocks."""
-    return n * shard // nshards, n * (shard + 1) // nshards
+SHARD_CHUNK = 32  # blocks per interleaved chunk, as the library splits query blocks
+
+
+def shard_items(n, shard, nshards, chunk=SHARD_CHUNK):
+    """Indices of shard `shard` of n items split over nshards the way
+    kd_count_radii_shard and kd_count_batch_shard split query blocks:
+    interleaved chunks of `chunk` items, chunk c to shard c mod nshards."""
+    idx = np.arange(n)
+    return idx[(idx // chunk) % nshards == shard]
 
 
 class Dist:

@@ -51,6 +51,7 @@ constexpr int kTileWarpsPerCta = 4;
 constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
 constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
+constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
 
 struct TreeSide {
     const double *x, *y, *z;
@@ -136,6 +137,7 @@ __device__ __forceinline__ void bin_range(const double *a, const double *b,
 // A tile record: x = run start, y = leaf, z = run length | tree field << 8 |
 // first active edge << 16 | active edge count << 24.
 struct TravOut {
+    const int *gmap;         // shard-local block index -> global block (NULL: identity)
     int *count;              // COUNT pass: tiles per block
     const long long *off;    // FILL pass: launch-relative tile offsets
     uint4 *rec;              // FILL: tile records
@@ -143,7 +145,7 @@ struct TravOut {
     int *err;
 };
 
-// one warp per global query block g in [g0, g1)
+// one warp per shard-local block index i in [g0, g1) (global block o.gmap[i])
 template <bool FILL>
 __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__restrict__ jobs,
                                                              const int *__restrict__ jblk,
@@ -157,8 +159,9 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
     for (int k = threadIdx.x; k < ne; k += blockDim.x) rsq[k] = g_rsq[k];
     __syncthreads();
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = g0 + blockIdx.x * kTravWarps + w;
-    if (g >= g1) return;
+    const int li = g0 + blockIdx.x * kTravWarps + w;
+    if (li >= g1) return;
+    const int g = o.gmap ? o.gmap[li] : li;
     const int j = job_of(jblk, njobs, g);
     const int b = g - jblk[j];
     const TreeSide T = jobs[j].T;
@@ -175,7 +178,7 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
     __syncwarp();
     int sp = 1;
     long long emitted = 0;
-    const long long base = FILL ? o.off[g - g0] : 0;
+    const long long base = FILL ? o.off[li - g0] : 0;
     unsigned long long acc_pairs = 0;
     long long guard = 4LL * T.nleaves + 64;
     while (sp > 0) {
@@ -276,7 +279,7 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
         emitted += etot;
         __syncwarp();
     }
-    if (!FILL && lane == 0) o.count[g - g0] = (int)emitted;
+    if (!FILL && lane == 0) o.count[li - g0] = (int)emitted;
     if (FILL) {
         for (int off = 16; off; off >>= 1) acc_pairs += __shfl_xor_sync(0xffffffffu, acc_pairs, off);
         if (lane == 0 && acc_pairs) atomicAdd(o.accepted, acc_pairs);
@@ -475,7 +478,8 @@ struct TileArgs {
     int njobs;
     const double *rsq;
     int ne;
-    int g0, g1;                 // global query blocks of this launch
+    int g0, g1;                 // shard-local block indices of this launch
+    const int *gmap;            // shard-local index -> global block (NULL: identity)
     const long long *off;       // launch-relative tile offsets
     const uint4 *rec;
     int *work;
@@ -513,8 +517,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
         int item = 0;
         if (lane == 0) item = atomicAdd(A.work, 1);
         item = __shfl_sync(0xffffffffu, item, 0);
-        const int g = A.g0 + item;
-        if (g >= A.g1) break;
+        const int li = A.g0 + item;
+        if (li >= A.g1) break;
+        const int g = A.gmap ? A.gmap[li] : li;
         const int jb = job_of(A.jblk, A.njobs, g);
         {
             const unsigned long long *src = (const unsigned long long *)(A.jobs + jb);
@@ -525,8 +530,8 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
         const JobDesc &J = ws->job;
         const int b = g - A.jblk[jb];
         const int qlen = J.Q.blk_len[b], qs = J.Q.blk_start[b];
-        const long long eoff = A.off[g - A.g0];
-        const int ecnt = (int)(A.off[g - A.g0 + 1] - eoff);
+        const long long eoff = A.off[li - A.g0];
+        const int ecnt = (int)(A.off[li - A.g0 + 1] - eoff);
         const double *bx = J.Q.blk_box + 6 * (size_t)b;
         const double ox = 0.5 * (bx[0] + bx[3]), oy = 0.5 * (bx[1] + bx[4]),
                      oz = 0.5 * (bx[2] + bx[5]);
@@ -1007,12 +1012,27 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
 
     // this shard's global blocks
     const int NB = hblk[njobs];
-    const int G0 = (int)((long long)NB * shard / nshards);
-    const int G1 = (int)((long long)NB * (shard + 1) / nshards);
+    // this shard's blocks: interleaved chunks of kShardChunk global blocks
+    // (chunk c belongs to shard c mod nshards), so that every shard gets an
+    // even mix of early and late blocks (a symmetric job's block only counts
+    // tree points after its own, so early blocks carry more work)
+    std::vector<int> gl;
+    if (nshards > 1)
+        for (int c = shard * kShardChunk; c < NB; c += nshards * kShardChunk)
+            for (int g = c; g < std::min(NB, c + kShardChunk); g++) gl.push_back(g);
+    const int G0 = 0;
+    const int G1 = nshards > 1 ? (int)gl.size() : NB;
     const int nb = G1 - G0;
+    int *gmap = nullptr;
+    if (nshards > 1 && nb > 0) {
+        gmap = pool.alloc<int>(nb);
+        check(cudaMemcpyAsync(gmap, gl.data(), sizeof(int) * (size_t)nb, cudaMemcpyHostToDevice, s),
+              "H2D");
+    }
     int *cnt = pool.alloc<int>(std::max(nb, 1));
     TravOut to;
     memset(&to, 0, sizeof to);
+    to.gmap = gmap;
     to.count = cnt;
     to.accepted = dstats + 2;
     to.err = err;
@@ -1085,6 +1105,7 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
         ta.ne = ne;
         ta.g0 = G0 + b0;
         ta.g1 = G0 + b1;
+        ta.gmap = gmap;
         ta.off = off;
         ta.rec = rec;
         ta.work = work;
@@ -1330,6 +1351,7 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
         ta.ne = ne;
         ta.g0 = b0;
         ta.g1 = b1;
+        ta.gmap = nullptr;
         ta.off = rel;
         ta.rec = rec;
         ta.work = err + 1;

@@ -118,8 +118,8 @@ void kdg_free(kd_catalog *cat);
  *              hist[e][qf][tf] = pairs whose FP64 squared distance d2
  *              satisfies rsq[e-1] <= d2 < rsq[e] (e = ne: beyond all edges,
  *              left zero)
- *   shard, nshards: count only query blocks [nb*shard/nshards,
- *              nb*(shard+1)/nshards) of the query catalog's nb blocks
+ *   shard, nshards: count only this shard's query blocks (interleaved
+ *              chunks of 32 blocks, chunk c on shard c mod nshards)
  */
 int kdg_count(const kd_catalog *tree, const kd_catalog *query,
               const double *rsq, int ne, int mode, int shard, int nshards,

@@ -133,11 +133,12 @@ void kd_free_counts(long long *counts);
 int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii,
                    int nradii, int mode, long long *out, kd_count_stats *stats);
 
-/* One shard of kd_count_radii: only the query points of query blocks
- * [nb*shard/nshards, nb*(shard+1)/nshards) are counted (nb: the query
- * tree's blocks of up to 128 spatially adjacent points).  Summing out over
- * all shards gives kd_count_radii's result exactly; one shard per GPU splits
- * a count across devices with no exchange until that final sum. */
+/* One shard of kd_count_radii: only the query points of this shard's query
+ * blocks are counted (the query tree's blocks of up to 128 spatially
+ * adjacent points, taken in interleaved chunks of 32: chunk c belongs to
+ * shard c mod nshards, which spreads early and late blocks evenly).  Summing
+ * out over all shards gives kd_count_radii's result exactly; one shard per
+ * GPU splits a count across devices with no exchange until that final sum. */
 int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii,
                          int nradii, int mode, int shard, int nshards,
                          long long *out, kd_count_stats *stats);
@@ -155,9 +156,9 @@ int kd_count_batch(const kdtree_t *trees, const kdtree_t *queries, int njobs,
                    const double *radii, int nradii, int mode, long long *out,
                    kd_count_stats *stats);
 
-/* One shard of kd_count_batch: blocks [nb*shard/nshards, nb*(shard+1)/nshards)
- * of the batch's nb global query blocks.  Summing out over all shards gives
- * kd_count_batch's result exactly. */
+/* One shard of kd_count_batch: the batch's query blocks (numbered job after
+ * job) split into interleaved chunks of 32 as in kd_count_radii_shard.
+ * Summing out over all shards gives kd_count_batch's result exactly. */
 int kd_count_batch_shard(const kdtree_t *trees, const kdtree_t *queries, int njobs,
                          const double *radii, int nradii, int mode, int shard,
                          int nshards, long long *out, kd_count_stats *stats);

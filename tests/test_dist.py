@@ -1,5 +1,5 @@
 """The multi-rank plumbing of bench.py on the CPU: two gloo ranks split the
-queries with bench.shard_range, count their share (the oracle stands in for
+queries with bench.shard_items (the library's interleaved split), count their share (the oracle stands in for
 the GPU counter here), SUM-reduce the int64 counts and MAX-reduce a timing.
 The reduced counts must equal the single-process count."""
 import os
@@ -29,8 +29,8 @@ def _rank_main(rank, world, port, out_path):
     f = (pts[:, 0] * 4).astype(np.int32)
     t = O.OracleTree(pts, f, 4)
     radii = np.logspace(-2, -0.8, 6)
-    lo, hi = bench.shard_range(len(pts), D.rank, D.world)
-    part = t.brute_counts(pts[lo:hi], f[lo:hi], 4, radii, nthreads=2)
+    idx = bench.shard_items(len(pts), D.rank, D.world, chunk=100)
+    part = t.brute_counts(pts[idx], f[idx], 4, radii, nthreads=2)
     total = D.reduce(part, "SUM")
     tmax = D.reduce([float(D.rank + 1)], "MAX")
     D.barrier()
@@ -48,10 +48,12 @@ def test_two_gloo_ranks_reduce_exact_counts(tmp_path):
     assert float(r["tmax"][0]) == 2.0
 
 
-def test_shard_range_partitions():
+def test_shard_items_partition():
     import bench
-    for n in (0, 1, 7, 156250):
+    for n in (0, 1, 7, 33, 156250):
         for k in (1, 2, 3, 8):
-            spans = [bench.shard_range(n, s, k) for s in range(k)]
-            assert spans[0][0] == 0 and spans[-1][1] == n
-            assert all(a[1] == b[0] for a, b in zip(spans, spans[1:]))
+            parts = [bench.shard_items(n, s, k) for s in range(k)]
+            allidx = np.sort(np.concatenate(parts))
+            assert np.array_equal(allidx, np.arange(n))  # disjoint and complete
+            if n >= 32 * k * 4:  # interleaved: every shard within one chunk of n/k
+                assert max(len(p) for p in parts) - min(len(p) for p in parts) <= 32
