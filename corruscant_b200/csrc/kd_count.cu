@@ -54,7 +54,6 @@ constexpr int kCoopMax = 32;            // rechecks of a run done by the whole w
 constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
 
 struct TreeSide {
-    const double *x, *y, *z;
     const double *box;
     const int *count, *tf, *leaf_run, *leaf_pos;
     const int *run_start, *run_len, *run_tf;
@@ -906,9 +905,6 @@ static JobDesc job_desc(const kd_catalog *tc, const kd_catalog *qc, unsigned lon
 {
     JobDesc d;
     memset(&d, 0, sizeof d);
-    d.T.x = tc->d_x;
-    d.T.y = tc->d_y;
-    d.T.z = tc->d_z;
     d.T.box = tc->d_box;
     d.T.count = tc->d_ncount;
     d.T.tf = tc->d_ntf;
