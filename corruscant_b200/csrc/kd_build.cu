@@ -35,6 +35,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <atomic>
 #include <exception>
 #include <new>
 #include <cmath>
@@ -64,19 +65,23 @@ constexpr int kSmallSeg = 256;
 // block touches at most two segments).
 constexpr int kVarChunk = 256;
 
+// Once per device (any thread may get here first; doing it twice is harmless):
+// keep freed stream-ordered allocations in the device's pool instead of
+// returning them to the driver at every synchronisation.
 void init_device()
 {
-    static int done_dev = -1;
+    static std::atomic<unsigned long long> done{0};
     int dev = 0;
     check(cudaGetDevice(&dev), "cudaGetDevice");
-    if (done_dev == dev) return;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0;
+    if (bit && (done.load() & bit)) return;
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
         uint64_t thr = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
     }
     cudaGetLastError();
-    done_dev = dev;
+    done.fetch_or(bit);
 }
 
 // Order-preserving 64-bit key of a double; -0.0 maps to +0.0's key so that
