@@ -581,7 +581,7 @@ def run_mine(args):
 # clustered workload at scale 0.3 summarised in profiles/, scaled to a full
 # launch by its pairs: the traffic is mostly the tile records, whose number
 # grows with the pairs.
-TILE_TRAFFIC_PER_PAIR = (3.319134e9 + 11.141376e6) / 2.02520e11  # bytes per pair tested
+TILE_TRAFFIC_PER_PAIR = (3.271633e9 + 11.673856e6) / 2.02520e11  # bytes per pair tested
 TILE_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_tiles launch, "
                        "clustered workload at scale 0.3 (2.025e11 pairs), scaled by pairs")
 
