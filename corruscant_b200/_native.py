@@ -93,6 +93,9 @@ def kdlib():
         L.kd_count_radii_shard.restype = c_int
         L.kd_count_radii_shard.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int, c_int,
                                            c_int, POINTER(c_longlong), POINTER(CountStats)]
+        L.kd_count_bins.restype = c_int
+        L.kd_count_bins.argtypes = [KdTree, KdTree, POINTER(c_double), c_int, c_int,
+                                    POINTER(c_longlong), POINTER(CountStats)]
         L.kd_count_batch_shard.restype = c_int
         L.kd_count_batch_shard.argtypes = [POINTER(KdTree), POINTER(KdTree), c_int, POINTER(c_double),
                                            c_int, c_int, c_int, c_int, POINTER(c_longlong),
@@ -184,6 +187,17 @@ def count_radii_shard(tree, query, radii, shard, nshards, mode=KD_MODE_MIXED, wi
     if rc != 0:
         raise_last()
     return (out, st.as_dict()) if with_stats else out
+
+
+def count_bins(tree, query, edges, mode=KD_MODE_MIXED):
+    """kd_count_bins: (len(edges)-1, Fq*Ft) per-bin counts."""
+    edges = np.require(np.asarray(edges, dtype=np.float64), requirements="AC")
+    out = np.zeros((max(0, len(edges) - 1), query.num_fields * tree.num_fields), dtype=np.int64)
+    rc = kdlib().kd_count_bins(tree, query, dptr(edges), c_int(len(edges)), c_int(mode),
+                               out.ctypes.data_as(POINTER(c_longlong)), None)
+    if rc != 0:
+        raise_last()
+    return out
 
 
 def count_batch(jobs, radii, mode=KD_MODE_MIXED, with_stats=False, shard=0, nshards=1):

@@ -406,6 +406,32 @@ int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii, int nradi
     return kd_count_radii_shard(tree, query, radii, nradii, mode, 0, 1, out, stats);
 }
 
+int kd_count_bins(kdtree_t tree, kdtree_t query, const double *edges, int nedges, int mode,
+                  long long *out, kd_count_stats *stats)
+{
+    long long *cum;
+    size_t nrow, k, j;
+    int rc;
+    clear_error();
+    if (nedges < 1 || !edges || !out) {
+        kd_set_error(KD_EINVAL, "kd_count_bins: need at least one edge");
+        return KD_EINVAL;
+    }
+    nrow = (size_t)(query.num_fields > 0 ? query.num_fields : 0) *
+           (size_t)(tree.num_fields > 0 ? tree.num_fields : 0);
+    cum = (long long *)malloc(sizeof(long long) * (nrow ? nrow : 1) * (size_t)nedges);
+    if (!cum) {
+        kd_set_error(KD_ENOMEM, "out of host memory");
+        return KD_ENOMEM;
+    }
+    rc = kd_count_radii(tree, query, edges, nedges, mode, cum, stats);
+    if (rc == KD_OK)
+        for (k = 0; k + 1 < (size_t)nedges; k++)
+            for (j = 0; j < nrow; j++) out[k * nrow + j] = cum[(k + 1) * nrow + j] - cum[k * nrow + j];
+    free(cum);
+    return rc;
+}
+
 int kd_count_batch_shard(const kdtree_t *trees, const kdtree_t *queries, int njobs,
                          const double *radii, int nradii, int mode, int shard, int nshards,
                          long long *out, kd_count_stats *stats)

@@ -143,6 +143,14 @@ int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii,
                          int nradii, int mode, int shard, int nshards,
                          long long *out, kd_count_stats *stats);
 
+/* Per-bin counts: out[k*Fq*Ft + qf*Fq + tf] = (count at edges[k+1]) -
+ * (count at edges[k]) for k = 0 .. nedges-2, exactly what the reference's
+ * drivers compute with np.diff over one pair_count per edge
+ * (clustering.py:218-230).  Edges in the caller's order (ascending for
+ * ordinary bins).  Returns 0 or a negative error code. */
+int kd_count_bins(kdtree_t tree, kdtree_t query, const double *edges, int nedges,
+                  int mode, long long *out, kd_count_stats *stats);
+
 /* kd_count_radii for njobs (trees[j], queries[j]) pairs sharing the radii
  * and mode, e.g. DD, DR and RR of an autocorrelation (clustering.py:218-230)
  * or the counts of many catalogs against one random catalog.  The query

@@ -188,6 +188,26 @@ def test_errors_are_reported_not_fatal():
         N.destroy(t)
 
 
+def test_count_bins_is_the_diff_of_per_edge_counts(golden):
+    """kd_count_bins gives the reference drivers' np.diff over per-edge counts
+    (the config-1 goldens are those per-bin arrays)."""
+    c1 = golden("config1.npz")
+    np.random.seed(3)
+    X = np.random.rand(4000, 3)
+    Y = np.random.rand(80000, 3)
+    td = _tree(X, (X[:, 0] * 4).astype("int32"), 4)
+    tr = _tree(Y, (Y[:, 0] * 4).astype("int32"), 4)
+    try:
+        for tree, query, key in ((td, td, "dd"), (tr, td, "dr"), (tr, tr, "rr")):
+            got = N.count_bins(tree, query, c1["radii"])
+            assert np.array_equal(got.reshape(-1, 4, 4), c1[key]), key
+        with pytest.raises(N.NativeError):
+            N.count_bins(td, td, [])
+    finally:
+        N.destroy(td)
+        N.destroy(tr)
+
+
 def test_shards_sum_to_full_count():
     """kd_count_radii_shard: the shards of the query blocks partition the
     count exactly (the multi-GPU split, run here on one device)."""
