@@ -1,0 +1,278 @@
+/*
+ * Host-library driver for the sanitizer tests: the real kd_api.c linked with
+ * the CPU stand-in of the device layer (fake_device.c).  Scenarios:
+ *   count   - the C ABI's counts against an independent brute force here
+ *             (radius order, repeats and NaN, query-major layout, batch
+ *             concatenation, per-bin differences, pair_count, the static
+ *             entry point);
+ *   threads - several threads building, counting and destroying trees at
+ *             once (run under ThreadSanitizer);
+ *   faults  - argument errors, injected device-layer failures and an
+ *             allocator that fails each allocation in turn (run under
+ *             AddressSanitizer, which also reports leaks).
+ * Prints PASS/FAIL lines; the exit status is the number of failures.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "kdtree.h"
+
+extern int fake_fail_build, fake_fail_count, fake_fail_copy;
+
+/* ---- allocator that can fail (kd_api.c's malloc/calloc/posix_memalign) */
+int fake_alloc_countdown = 0;
+static pthread_mutex_t alloc_mu = PTHREAD_MUTEX_INITIALIZER;
+static int alloc_should_fail(void)
+{
+    int fail = 0;
+    pthread_mutex_lock(&alloc_mu);
+    if (fake_alloc_countdown > 0 && --fake_alloc_countdown == 0) fail = 1;
+    pthread_mutex_unlock(&alloc_mu);
+    return fail;
+}
+void *fake_malloc(size_t n) { return alloc_should_fail() ? NULL : malloc(n); }
+void *fake_calloc(size_t c, size_t s) { return alloc_should_fail() ? NULL : calloc(c, s); }
+int fake_posix_memalign(void **p, size_t a, size_t n)
+{
+    if (alloc_should_fail()) return 12; /* ENOMEM */
+    return posix_memalign(p, a, n);
+}
+
+static int failures = 0;
+#define CHECK(cond, ...)                                  \
+    do {                                                  \
+        if (!(cond)) {                                    \
+            failures++;                                   \
+            printf("FAIL %s:%d: ", __FILE__, __LINE__);   \
+            printf(__VA_ARGS__);                          \
+            printf("\n");                                 \
+        }                                                 \
+    } while (0)
+
+static unsigned long long rng = 88172645463325252ull;
+static double urand(void)
+{
+    rng ^= rng << 13;
+    rng ^= rng >> 7;
+    rng ^= rng << 17;
+    return (double)(rng >> 11) * (1.0 / 9007199254740992.0);
+}
+
+typedef struct {
+    double *xyz;
+    int *f;
+    int n, nf;
+} cat_t;
+
+static cat_t make_cat(int n, int nf)
+{
+    cat_t c;
+    int i;
+    c.n = n;
+    c.nf = nf;
+    c.xyz = (double *)malloc(sizeof(double) * 3 * (size_t)n);
+    c.f = (int *)malloc(sizeof(int) * (size_t)n);
+    for (i = 0; i < 3 * n; i++) c.xyz[i] = urand();
+    for (i = 0; i < n; i++) c.f[i] = (int)(c.xyz[3 * i] * nf) % nf;
+    return c;
+}
+
+/* expected out[k][qf*Fq + tf] for radius k: the reference's pair_count */
+static void brute(const cat_t *t, const cat_t *q, const double *radii, int nr, long long *out)
+{
+    int k, i, j;
+    const int Fq = q->nf, Ft = t->nf;
+    memset(out, 0, sizeof(long long) * (size_t)nr * Fq * Ft);
+    for (k = 0; k < nr; k++) {
+        const double rsq = radii[k] * radii[k];
+        for (i = 0; i < q->n; i++)
+            for (j = 0; j < t->n; j++) {
+                const double *a = t->xyz + 3 * j, *b = q->xyz + 3 * i;
+                const double dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+                const double d2 = fma(dz, dz, fma(dy, dy, dx * dx));
+                if (d2 < rsq) out[(size_t)k * Fq * Ft + (size_t)q->f[i] * Fq + t->f[j]]++;
+            }
+    }
+}
+
+static int same(const long long *a, const long long *b, size_t n)
+{
+    return memcmp(a, b, sizeof(long long) * n) == 0;
+}
+
+static const double RADII[] = {0.3, 0.05, NAN, 0.2, 0.05, 0.0, INFINITY, 0.12};
+#define NR ((int)(sizeof RADII / sizeof RADII[0]))
+
+static void scenario_count(void)
+{
+    cat_t a = make_cat(300, 3), b = make_cat(500, 3);
+    kdtree_t ta = tree_construct(a.xyz, a.f, a.n, a.nf), tb = tree_construct(b.xyz, b.f, b.n, b.nf);
+    long long want[3][NR * 9], got[3 * NR * 9], cum[NR * 9];
+    kdtree_t trees[3] = {ta, tb, tb}, queries[3] = {ta, ta, tb};
+    const cat_t *tc[3] = {&a, &b, &b}, *qc[3] = {&a, &a, &b};
+    int j, k;
+    CHECK(ta.node_data && tb.node_data, "tree_construct failed");
+    for (j = 0; j < 3; j++) {
+        brute(tc[j], qc[j], RADII, NR, want[j]);
+        CHECK(kd_count_radii(trees[j], queries[j], RADII, NR, KD_MODE_MIXED, got, NULL) == 0,
+              "kd_count_radii");
+        CHECK(same(got, want[j], NR * 9), "kd_count_radii job %d differs", j);
+    }
+    CHECK(kd_count_batch(trees, queries, 3, RADII, NR, KD_MODE_FP64, got, NULL) == 0,
+          "kd_count_batch");
+    for (j = 0; j < 3; j++) CHECK(same(got + j * NR * 9, want[j], NR * 9), "batch job %d", j);
+    {
+        const double edges[] = {0.0, 0.05, 0.12, 0.2, 0.3};
+        long long bins[4 * 9], e_cum[5 * 9];
+        brute(&b, &a, edges, 5, e_cum);
+        CHECK(kd_count_bins(tb, ta, edges, 5, KD_MODE_MIXED, bins, NULL) == 0, "kd_count_bins");
+        for (k = 0; k < 4 * 9; k++) CHECK(bins[k] == e_cum[k + 9] - e_cum[k], "bin %d", k);
+    }
+    {
+        long long *p = pair_count(tb, a.xyz, a.f, a.n, 3, 0.2, 4);
+        brute(&b, &a, (const double[]){0.2}, 1, cum);
+        CHECK(p && same(p, cum, 9), "pair_count");
+        kd_free_counts(p);
+    }
+    CHECK(kd_count_radii_static(tb, ta, RADII, NR, KD_MODE_MIXED, got) == 0, "static");
+    CHECK(same(got, want[1], NR * 9), "static differs");
+    destroy(ta);
+    destroy(tb);
+    destroy(ta); /* a second destroy of the same tree is a no-op */
+    free(a.xyz), free(a.f), free(b.xyz), free(b.f);
+    printf("PASS count\n");
+}
+
+/* ---- threads */
+static cat_t g_cat;
+static long long g_want[NR * 4];
+static void *worker(void *arg)
+{
+    int it;
+    (void)arg;
+    for (it = 0; it < 40; it++) {
+        long long got[NR * 4];
+        char msg[128];
+        kdtree_t t = tree_construct(g_cat.xyz, g_cat.f, g_cat.n, g_cat.nf);
+        if (!t.node_data) {
+            CHECK(0, "threaded tree_construct");
+            continue;
+        }
+        CHECK(kd_count_radii(t, t, RADII, NR, it & 1, got, NULL) == 0, "threaded count");
+        CHECK(same(got, g_want, NR * 4), "threaded count differs");
+        /* errors stay per thread */
+        CHECK(kd_count_radii(t, t, (const double[]){-1.0}, 1, 0, got, NULL) < 0, "neg radius");
+        CHECK(kd_last_error(msg, sizeof msg) < 0 && strstr(msg, "negative"), "thread error: %s", msg);
+        destroy(t);
+    }
+    return NULL;
+}
+
+static void scenario_threads(void)
+{
+    pthread_t th[8];
+    int i;
+    g_cat = make_cat(200, 2);
+    brute(&g_cat, &g_cat, RADII, NR, g_want);
+    for (i = 0; i < 8; i++) pthread_create(&th[i], NULL, worker, NULL);
+    for (i = 0; i < 8; i++) pthread_join(th[i], NULL);
+    free(g_cat.xyz), free(g_cat.f);
+    printf("PASS threads\n");
+}
+
+/* ---- faults */
+static int sequence(const cat_t *a)
+{
+    /* a whole use of the library; returns the number of calls that failed */
+    int bad = 0;
+    long long out[NR * 4], *p;
+    kdtree_t t = tree_construct(a->xyz, a->f, a->n, a->nf), trees[2], qs[2];
+    if (!t.node_data) return 1;
+    bad += kd_count_radii(t, t, RADII, NR, 0, out, NULL) != 0;
+    trees[0] = trees[1] = qs[0] = qs[1] = t;
+    {
+        long long big[2 * NR * 4];
+        bad += kd_count_batch(trees, qs, 2, RADII, NR, 0, big, NULL) != 0;
+    }
+    p = pair_count(t, a->xyz, a->f, a->n, a->nf, 0.1, 1);
+    bad += p == NULL;
+    kd_free_counts(p);
+    bad += kd_count_points(t, a->xyz, a->f, a->n, a->nf, RADII, NR, 0, out, NULL) != 0;
+    destroy(t);
+    return bad;
+}
+
+static void scenario_faults(void)
+{
+    cat_t a = make_cat(150, 2);
+    long long out[NR * 4];
+    kdtree_t t;
+    int n, code, okruns = 0;
+    char msg[128];
+
+    /* argument errors */
+    t = tree_construct(a.xyz, a.f, a.n, a.nf);
+    CHECK(kd_count_radii(t, t, RADII, NR, 5, out, NULL) < 0, "bad mode");
+    CHECK(kd_count_radii_shard(t, t, RADII, NR, 0, 2, 2, out, NULL) < 0, "bad shard");
+    CHECK(kd_set_precision(9) < 0 && kd_set_precision(KD_MODE_FP64) == 0, "precision");
+    kd_set_precision(KD_MODE_MIXED);
+    CHECK(kd_set_device(3) < 0, "device");
+    {
+        double r[65];
+        long long o65[65 * 4];
+        for (n = 0; n < 65; n++) r[n] = 0.001 * (n + 1);
+        CHECK(kd_count_radii(t, t, r, 65, 0, o65, NULL) < 0, "65 distinct radii accepted");
+        CHECK(kd_count_radii(t, t, r, 64, 0, o65, NULL) == 0, "64 distinct radii refused");
+        CHECK(kd_count_radii(t, t, (const double[]){0.1, -0.1}, 2, 0, o65, NULL) < 0, "neg");
+    }
+    destroy(t);
+
+    /* injected device-layer failures: clean errors, nothing leaks */
+    fake_fail_build = -2;
+    t = tree_construct(a.xyz, a.f, a.n, a.nf);
+    code = kd_last_error(msg, sizeof msg);
+    CHECK(!t.node_data && code == -2 && strstr(msg, "injected"), "build failure: %d %s", code, msg);
+    fake_fail_build = 0;
+    fake_fail_copy = -6;
+    t = tree_construct(a.xyz, a.f, a.n, a.nf);
+    CHECK(!t.node_data && kd_last_error(NULL, 0) == -6, "copy failure");
+    fake_fail_copy = 0;
+    t = tree_construct(a.xyz, a.f, a.n, a.nf);
+    fake_fail_count = -8;
+    CHECK(kd_count_radii(t, t, RADII, NR, 0, out, NULL) == -8, "count failure");
+    CHECK(pair_count(t, a.xyz, a.f, a.n, a.nf, 0.1, 1) == NULL, "pair_count failure");
+    fake_fail_count = 0;
+    destroy(t);
+
+    /* every allocation of a whole sequence failing in turn */
+    for (n = 1; n < 200; n++) {
+        int bad;
+        fake_alloc_countdown = n;
+        bad = sequence(&a);
+        if (fake_alloc_countdown > 0) { /* the n-th allocation was never reached */
+            fake_alloc_countdown = 0;
+            CHECK(bad == 0, "sequence failed without an injected failure");
+            okruns++;
+            break;
+        }
+        CHECK(bad > 0, "allocation %d failed but every call succeeded", n);
+    }
+    CHECK(okruns == 1 && n > 5, "allocation sweep ended after %d steps", n);
+    free(a.xyz), free(a.f);
+    printf("PASS faults (%d allocation points)\n", n - 1);
+}
+
+int main(int argc, char **argv)
+{
+    int i;
+    for (i = 1; i < argc; i++) {
+        if (!strcmp(argv[i], "count")) scenario_count();
+        else if (!strcmp(argv[i], "threads")) scenario_threads();
+        else if (!strcmp(argv[i], "faults")) scenario_faults();
+    }
+    printf("%d failures\n", failures);
+    return failures;
+}
