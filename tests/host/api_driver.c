@@ -9,7 +9,9 @@
  *             once (run under ThreadSanitizer);
  *   faults  - argument errors, injected device-layer failures and an
  *             allocator that fails each allocation in turn (run under
- *             AddressSanitizer, which also reports leaks).
+ *             AddressSanitizer, which also reports leaks);
+ *   coords  - the threaded RA/DEC conversion (coords_api.c), three callers
+ *             at once, against a single-threaded evaluation.
  * Prints PASS/FAIL lines; the exit status is the number of failures.
  */
 #include <math.h>
@@ -18,6 +20,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include "coordmath.h"
 #include "kdtree.h"
 
 extern int fake_fail_build, fake_fail_count, fake_fail_copy;
@@ -265,6 +268,46 @@ static void scenario_faults(void)
     printf("PASS faults (%d allocation points)\n", n - 1);
 }
 
+/* ---- coords: the threaded host conversion against a single-threaded
+ * evaluation of the reference's formula (coordmath.c:38-51), from several
+ * callers at once */
+#define NC 1000000
+static double *c_ra, *c_dec, *c_want;
+static void *coord_worker(void *arg)
+{
+    double *xyz = (double *)malloc(sizeof(double) * 3 * NC);
+    (void)arg;
+    radec2cart64(c_ra, c_dec, xyz, NC);
+    CHECK(memcmp(xyz, c_want, sizeof(double) * 3 * NC) == 0, "threaded radec2cart64 differs");
+    free(xyz);
+    return NULL;
+}
+
+static void scenario_coords(void)
+{
+    const double d2r = M_PI / 180.0;
+    pthread_t th[3];
+    int i;
+    c_ra = (double *)malloc(sizeof(double) * NC);
+    c_dec = (double *)malloc(sizeof(double) * NC);
+    c_want = (double *)malloc(sizeof(double) * 3 * NC);
+    for (i = 0; i < NC; i++) {
+        double lon, lat, c;
+        c_ra[i] = 360.0 * urand();
+        c_dec[i] = 180.0 * urand() - 90.0;
+        lon = c_ra[i] * d2r;
+        lat = c_dec[i] * d2r;
+        c = cos(lat);
+        c_want[3 * i] = c * cos(lon);
+        c_want[3 * i + 1] = c * sin(lon);
+        c_want[3 * i + 2] = sin(lat);
+    }
+    for (i = 0; i < 3; i++) pthread_create(&th[i], NULL, coord_worker, NULL);
+    for (i = 0; i < 3; i++) pthread_join(th[i], NULL);
+    free(c_ra), free(c_dec), free(c_want);
+    printf("PASS coords\n");
+}
+
 int main(int argc, char **argv)
 {
     int i;
@@ -272,6 +315,7 @@ int main(int argc, char **argv)
         if (!strcmp(argv[i], "count")) scenario_count();
         else if (!strcmp(argv[i], "threads")) scenario_threads();
         else if (!strcmp(argv[i], "faults")) scenario_faults();
+        else if (!strcmp(argv[i], "coords")) scenario_coords();
     }
     printf("%d failures\n", failures);
     return failures;

@@ -3,7 +3,8 @@
 tests/host/fake_device.c stands in for the device layer (an exhaustive CPU
 count over the stored points); tests/host/api_driver.c drives the real C
 ABI: counts against an independent brute force, eight threads building,
-counting and destroying trees at once under ThreadSanitizer, and argument
+counting and destroying trees at once and three callers of the threaded
+RA/DEC conversion under ThreadSanitizer, and argument
 errors, injected device-layer failures and every allocation failing in turn
 under AddressSanitizer + UndefinedBehaviorSanitizer (leaks included)."""
 import os
@@ -28,7 +29,8 @@ def _build(tmp_path, sanitize, tag):
         ["gcc", *flags, *inc, "-include", os.path.join(SRC, "fake_alloc.h"), "-c",
          os.path.join(REPO, "corruscant_b200", "csrc", "kd_api.c"), "-o", obj],
         ["gcc", *flags, *inc, os.path.join(SRC, "fake_device.c"), os.path.join(SRC, "api_driver.c"),
-         obj, "-o", exe, "-lpthread", "-lm"],
+         os.path.join(REPO, "corruscant_b200", "csrc", "coords_api.c"), obj, "-o", exe,
+         "-lpthread", "-lm"],
     ]
     for c in cmds:
         r = subprocess.run(c, capture_output=True, text=True)
@@ -49,8 +51,8 @@ def _run(exe, *scenarios, env=None):
 
 def test_host_library_under_thread_sanitizer(tmp_path):
     exe = _build(tmp_path, "thread", "tsan")
-    out = _run(exe, "threads", "count", env={"TSAN_OPTIONS": "halt_on_error=1"})
-    assert "PASS threads" in out and "PASS count" in out
+    out = _run(exe, "threads", "count", "coords", env={"TSAN_OPTIONS": "halt_on_error=1"})
+    assert "PASS threads" in out and "PASS count" in out and "PASS coords" in out
 
 
 def test_host_library_under_address_sanitizer(tmp_path):
