@@ -109,6 +109,35 @@ def test_mock_catalogs_against_shared_randoms():
             N.destroy(m)
 
 
+def test_many_tiny_jobs_in_one_batch():
+    """Hundreds of catalogs of 1..50 points in one batch (most jobs are a
+    single query block): every job still gets exactly its own counts."""
+    rs = np.random.RandomState(24)
+    cats = []
+    for i in range(300):
+        n = int(rs.randint(1, 51))
+        p = rs.rand(n, 3)
+        nf = int(rs.randint(1, 4))
+        f = (p[:, 0] * nf).astype(np.int32).clip(0, nf - 1) if nf > 1 else None
+        cats.append((p, f, nf))
+    trees = [N.build_tree(p, f, nf) for p, f, nf in cats]
+    radii = np.array([0.0, 0.05, 0.2, 0.5, np.inf])
+    try:
+        pairs = [(i, i) for i in range(300)] + \
+                [(i, (7 * i + 3) % 300) for i in range(0, 300, 3)
+                 if cats[i][2] == cats[(7 * i + 3) % 300][2]]
+        got = N.count_batch([(trees[ti], trees[qi]) for ti, qi in pairs], radii)
+        assert len(got) == len(pairs)
+        for (ti, qi), g in zip(pairs, got):
+            pt, ft, nft = cats[ti]
+            pq, fq, nfq = cats[qi]
+            want = O.OracleTree(pt, ft, nft).brute_counts(pq, fq, nfq, radii, nthreads=1)
+            assert np.array_equal(g, want), (ti, qi)
+    finally:
+        for t in trees:
+            N.destroy(t)
+
+
 def test_batch_argument_errors():
     rs = np.random.RandomState(1)
     t = N.build_tree(rs.rand(100, 3), None, 1)

@@ -85,6 +85,24 @@ def test_concurrent_counts_from_threads():
         N.destroy(b)
 
 
+@pytest.mark.parametrize("offset", [1.0e6, -3.0e4])
+def test_far_from_origin(offset):
+    """Coordinates of ~1e6 with separations of ~1e-4: FP32 values of the
+    coordinates themselves would be useless here; the tile kernel works on
+    block-relative coordinates and must still count exactly."""
+    rs = np.random.RandomState(46)
+    p = offset + rs.rand(20000, 3) * 0.01
+    f = (rs.rand(len(p)) * 3).astype(np.int32)
+    t = N.build_tree(p, f, 3)
+    try:
+        radii = np.array([1e-4, 3e-4, 1e-3, 2e-3, 5e-3])
+        want = O.OracleTree(p, f, 3).brute_counts(p, f, 3, radii, nthreads=8)
+        for mode in (N.KD_MODE_MIXED, N.KD_MODE_FP64):
+            assert np.array_equal(N.count_radii(t, t, radii, mode=mode), want)
+    finally:
+        N.destroy(t)
+
+
 def test_fields_above_255_follow_the_reference():
     """The tree side keeps the low 8 bits of a field id (kdtree.h field:8), the
     query side the full id; an autocorrelation with such fields is counted the
