@@ -52,6 +52,10 @@ constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flus
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
 constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
 constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
+constexpr int kRunPerLane = KD_RUN_MAX / 32;  // staged run points per lane
+// A run's exact counts travel one per byte (recounts) and its FP32 band sums
+// stay small (at most 4 * KD_RUN_MAX terms in [0, 1]): both need short runs.
+static_assert(KD_RUN_MAX % 32 == 0 && KD_RUN_MAX <= 128, "runs of 32..128 points");
 
 struct TreeSide {
     const double *box;
@@ -326,7 +330,9 @@ __device__ __forceinline__ float fma_sat(float a, float b, float c)
 // Each pair gives c = sat(a_k + s * nsl_k): exactly 0 or 1 outside the band,
 // in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals acc2 = sum c^2 bit
 // for bit when every c is 0 or 1; a band pair makes them differ by at least
-// 3/16, far above the FP32 rounding of these short sums (<= 256 terms <= 1).
+// 3/16, far above the FP32 rounding of these short sums (at most
+// 4 * KD_RUN_MAX <= 512 terms in [0, 1]: each sum is off by at most
+// 512 * 512 * 2^-24 = 1/64).
 // Queries travel in pairs through the packed FP32 pipe (FFMA2/FADD2: two
 // independent round-to-nearest operations per instruction, the same values
 // as the scalar chain); the saturating ramp has no packed form and stays
@@ -433,9 +439,10 @@ __device__ __forceinline__ void fp64_run(const double *__restrict__ tx,
 }
 
 // Warp-cooperative exact recount of one query over a run: every lane takes
-// the points j = lane, lane + 32 (at most two, so each lane's per-edge count
-// is at most 2 and the warp sum at most 64: the four byte-packed counts add
-// without carries in one reduction).  Returns the packed counts in all lanes.
+// the points j = lane, lane + 32, ... (at most KD_RUN_MAX / 32, so the warp
+// sum of each per-edge count is at most KD_RUN_MAX <= 128: the four
+// byte-packed counts add without carries in one reduction).  Returns the
+// packed counts in all lanes.
 __device__ __noinline__ unsigned exact_pass_warp(const double *__restrict__ tx,
                                                  const double *__restrict__ ty,
                                                  const double *__restrict__ tz, int rl,
@@ -657,7 +664,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
         // the next record's loads, held in registers while the current run
         // is counted
         uint4 nrec = make_uint4(0, 0, 0, 0);
-        float4 na = make_float4(0, 0, 0, 0), nb = na;
+        float4 npt[kRunPerLane];
+#pragma unroll
+        for (int h = 0; h < kRunPerLane; h++) npt[h] = make_float4(0, 0, 0, 0);
         double ncx = 0, ncy = 0, ncz = 0;
         auto issue = [&](int i) {
             nrec = A.rec[eoff + i];
@@ -668,8 +677,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                 ncx = J.leaf_c[3 * (size_t)leaf];
                 ncy = J.leaf_c[3 * (size_t)leaf + 1];
                 ncz = J.leaf_c[3 * (size_t)leaf + 2];
-                if (lane < rl) na = J.t4[rs + lane];
-                if (lane + 32 < rl) nb = J.t4[rs + lane + 32];
+#pragma unroll
+                for (int h = 0; h < kRunPerLane; h++)
+                    if (lane + 32 * h < rl) npt[h] = J.t4[rs + lane + 32 * h];
             } else {
                 const unsigned rs = nrec.x;
                 if (lane < rl) {
@@ -689,15 +699,14 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             if (K != 0) {
                 if (MODE == KD_MODE_MIXED) {
                     const float dx = (float)(ncx - ox), dy = (float)(ncy - oy), dz = (float)(ncz - oz);
-                    const float4 v2[2] = {na, nb};
 #pragma unroll
-                    for (int h = 0; h < 2; h++) {
+                    for (int h = 0; h < kRunPerLane; h++) {
                         const int j = lane + 32 * h;
                         if (j < rl) {
                             // t' = t_r + (c - o); -0.5 * (-2 t_r) is exact
-                            const float lx = fmaf(-0.5f, v2[h].x, dx);
-                            const float ly = fmaf(-0.5f, v2[h].y, dy);
-                            const float lz = fmaf(-0.5f, v2[h].z, dz);
+                            const float lx = fmaf(-0.5f, npt[h].x, dx);
+                            const float ly = fmaf(-0.5f, npt[h].y, dy);
+                            const float lz = fmaf(-0.5f, npt[h].z, dz);
                             const float X = -2.0f * lx, Y = -2.0f * ly, Z = -2.0f * lz;
                             const float N = fmaf(lz, lz, fmaf(ly, ly, lx * lx));
                             ws->stage[2 * j] = make_float4(X, X, Y, Y);

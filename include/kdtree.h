@@ -99,7 +99,7 @@ typedef struct kd_count_stats {
     long long pairs_accepted;  /* pairs binned by whole node pairs, no distance */
     long long pairs_wide;      /* pairs of tiles spanning more than 4 edges */
     long long edge_pairs;      /* sum over tested pairs of the edges each was binned against */
-    long long warp_tiles;      /* (32 queries, tree run) tiles computed */
+    long long warp_tiles;      /* (query block, tree run) tiles with distances computed */
     long long entries;         /* (query block, tree run) tiles listed */
     double ms_traverse;        /* device time: node-pair traversal */
     double ms_tiles;           /* device time: tile kernels */
