@@ -49,6 +49,28 @@ def test_reference_arm_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+def test_reference_arm_under_torchrun_prints_once():
+    """Launched like the multi-GPU runs (torchrun, 2 ranks): rank 0 alone
+    runs the CPU reference and prints one line; the other rank exits 0."""
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = subprocess.run(
+        [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+         "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl",
+         "reference", "--gpus", "2", "--scale", "0.01", "--steps", "1", "--warmup", "0",
+         "--cpu-queries", "200"],
+        capture_output=True, text=True, timeout=600, cwd=HERE)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, out.stdout[-2000:]
+    d = json.loads(lines[0])
+    _check_base(d)
+    assert d["impl"] == "reference" and d["n_gpus"] == 2
+
+
 @pytest.mark.gpu
 def test_gpu_arm_line():
     d = _run("--scale", "0.01", "--steps", "1", "--warmup", "3", "--cpu-queries", "200")
