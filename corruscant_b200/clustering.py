@@ -258,6 +258,26 @@ class results(object):
                 arr /= _grid_sum(a, b).astype("float64")
         return kept
 
+    def _jackknife_all(self, normalized):
+        """``jackknife_pair_counts(f, normalized)`` for every field f at once,
+        as (bins, F) arrays.  The counts kept without field f are total - row
+        f - column f + cell (f, f), and the normalisation is the product of
+        the field-size sums without f: both exact integers (int64), so every
+        element equals the per-field method's, which zeroes a copy and sums
+        it (clustering.py:457-491).  Integer count arrays only."""
+        out = []
+        for arr, (a, b) in zip(self.count_arrays, self.count_sizes):
+            tot = np.sum(arr, axis=(1, 2))
+            kept = (tot[:, np.newaxis] - np.sum(arr, axis=2) - np.sum(arr, axis=1) +
+                    np.diagonal(arr, axis1=1, axis2=2))
+            if normalized:
+                a = np.asarray(a, dtype=np.int64)
+                b = np.asarray(b, dtype=np.int64)
+                den = (np.sum(a) - a) * (np.sum(b) - b)
+                kept = kept.astype("float64") / den.astype("float64")[np.newaxis, :]
+            out.append(kept)
+        return out
+
     def bootstrap_pair_counts(self, N_trials):
         """Estimator inputs for N_trials field resamplings (numpy's global
         random state, as in clustering.py:416-455): (bins, N_trials) each."""
@@ -308,6 +328,21 @@ class results(object):
         cov = np.zeros((self.nbins, self.nbins))
         xi = self.estimate()
         tot_rr = self.total_pair_counts(normalized=False)[-1].astype("float64")
+        if jack and all(np.issubdtype(np.asarray(c).dtype, np.integer)
+                        for c in self.count_arrays):
+            # all fields at once (elementwise, so bit-identical to the loop
+            # below); the sum over fields keeps its order
+            est = self.estimator(*self._jackknife_all(normalized=True))
+            raw = self._jackknife_all(normalized=False)[-1]
+            diffs = est - xi[:, np.newaxis]
+            ws = np.sqrt(raw / tot_rr[:, np.newaxis])
+            for fid in range(self.N_fields):
+                diff, w = diffs[:, fid], ws[:, fid]
+                cov += (w * diff)[np.newaxis, :] * w[:, np.newaxis] * diff[:, np.newaxis]
+            if normalized:
+                sig = np.sqrt(np.diagonal(cov))
+                return np.divide(cov, sig[np.newaxis, :] * sig[:, np.newaxis])
+            return cov
         for fid in range(self.N_fields):
             if jack:
                 norm = self.jackknife_pair_counts(fid, normalized=True)

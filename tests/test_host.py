@@ -86,6 +86,36 @@ def test_crosscorr_estimators_match_reference_to_0ulp(golden):
     _check_estimators(res, g)
 
 
+@pytest.mark.parametrize("est", ["landy-szalay", "hamilton", "standard"])
+@pytest.mark.parametrize("cross", [False, True])
+def test_jackknife_covariance_at_100_fields_equals_the_per_field_loop(est, cross):
+    """The all-fields jackknife covariance (exact integer counts kept per
+    field) is bit for bit the reference's loop over fields built on
+    jackknife_pair_counts(f) (clustering.py:520-558), at F = 100."""
+    rs = np.random.RandomState(21 + cross)
+    F, nb = 100, 15
+    arrays = [rs.randint(0, 10 ** k, (nb, F, F)).astype(np.int64) for k in (5, 6, 7, 8)]
+    arrays = arrays if cross else arrays[:3]
+    arrays[-1] += 1
+    s = [rs.randint(1, 10 ** 5, F) for _ in range(4)]
+    res = clustering.results.__new__(clustering.results)
+    clustering.results.__init__(res, clustering._estimator(est), np.logspace(-3, 0, nb + 1))
+    res.count_arrays, res.N_fields = arrays, F
+    res.count_sizes = ([(s[0], s[1]), (s[0], s[3]), (s[1], s[2]), (s[2], s[3])] if cross
+                       else [(s[0], s[0]), (s[0], s[1]), (s[1], s[1])])
+    xi = res.estimate()
+    tot_rr = res.total_pair_counts(normalized=False)[-1].astype("float64")
+    want = np.zeros((nb, nb))
+    for fid in range(F):
+        diff = res.estimator(*res.jackknife_pair_counts(fid, normalized=True)) - xi
+        w = np.sqrt(res.jackknife_pair_counts(fid, normalized=False)[-1] / tot_rr)
+        want += (w * diff)[np.newaxis, :] * w[:, np.newaxis] * diff[:, np.newaxis]
+    _assert_bits(res.covariance("jackknife"), want)
+    sig = np.sqrt(np.diagonal(want))
+    _assert_bits(res.covariance("jackknife", normalized=True),
+                 np.divide(want, sig[np.newaxis, :] * sig[:, np.newaxis]))
+
+
 def test_results_table_prints():
     dd = np.arange(1, 9).reshape(2, 2, 2)
     res = clustering.autocorr_results(dd, dd + 1, dd + 2, _fake_tree(np.array([0, 1]), 2),
