@@ -5,7 +5,9 @@ Runs only where the reference sources are available: it needs
 into oracle/_ref/) and, for the estimator values, the reference's Python
 package, which it imports from a temporary copy of the reference tree.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [--only=PART,...]
+
+(PART: trees, estimators, coords, alltypes; default all.)
 
 Outputs (all small):
   trees.npz        inputs + reference node arrays (semantic fields) for small
@@ -16,7 +18,12 @@ Outputs (all small):
                    DD/DR/RR per bin and the reference estimator / error values
   cross.npz        a small cross-correlation with the reference's estimators
   coords.npz       reference radec2cart64 / radecdist2cart64 outputs
+  alltypes.npz     the workloads of the reference's test/test_alltypes.py
+                   (3-D and angular, auto and cross, with and without
+                   fields; seeded inputs): counts, every estimator x error
+                   type and the reference's printed results tables
 """
+import hashlib
 import os
 import shutil
 import sys
@@ -82,6 +89,21 @@ def main():
     if not O.ref_available():
         sys.exit("build the reference first: make -C oracle ref")
     R = O.RefLib()
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = [a.split("=", 1)[1].split(",") for a in sys.argv[1:] if a.startswith("--only=")]
+    parts = set(only[0]) if only else {"trees", "estimators", "coords", "alltypes"}
+    ref_root = args[0] if args else "/root/reference"
+    if "trees" in parts:
+        make_tree_goldens(R)
+    if "estimators" in parts:
+        make_estimator_goldens(R, ref_root)
+    if "coords" in parts:
+        make_coord_goldens(R)
+    if "alltypes" in parts:
+        make_alltypes_goldens(R, ref_root)
+
+
+def make_tree_goldens(R):
     trees, counts = {}, {}
     rs = np.random.RandomState(7)
     for name, (p, f, nf) in point_sets().items():
@@ -135,14 +157,15 @@ def main():
     np.savez_compressed(os.path.join(HERE, "trees.npz"), **trees)
     np.savez_compressed(os.path.join(HERE, "counts.npz"), **counts)
 
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    make_estimator_goldens(R, ref_root)
-    make_coord_goldens(R)
+
+_REF_PY = {}
 
 
 def _ref_python(ref_root):
     """Import the reference's Python package from a temporary copy whose bin/
     holds the libraries compiled from the reference sources."""
+    if "clustering" in _REF_PY:
+        return _REF_PY["clustering"]
     tmp = tempfile.mkdtemp(prefix="refpy_")
     shutil.copytree(os.path.join(ref_root, "corruscant"), os.path.join(tmp, "corruscant"))
     os.makedirs(os.path.join(tmp, "corruscant", "bin"), exist_ok=True)
@@ -150,6 +173,7 @@ def _ref_python(ref_root):
         shutil.copy(os.path.join(O.ref_path(), lib), os.path.join(tmp, "corruscant", "bin", lib))
     sys.path.insert(0, tmp)
     import corruscant.clustering as clustering  # noqa: E402
+    _REF_PY["clustering"] = clustering
     return clustering
 
 
@@ -222,6 +246,120 @@ def make_estimator_goldens(R, ref_root):
                         radii=radii, d1d2=d1d2, d1r2=d1r2, d2r1=d2r1, r1r2=r1r2, **vals)
     for t in trs:
         R.destroy(t)
+
+
+# ------------------------------------------------ test/test_alltypes.py cases
+
+ALLTYPES_ESTIMATORS = ("standard", "hamilton", "landy-szalay")
+ALLTYPES_ERRORS = (None, "poisson", "ftf", "jackknife", "bootstrap")
+ALLTYPES_CASES = {
+    # name: (auto | cross, cube | sphere, catalog sizes, eight fields?, seed)
+    "cube_nofield": ("auto", "cube", (4000, 80000), False, 41),
+    "cube_fields": ("auto", "cube", (4000, 80000), True, 42),
+    "cube_cross": ("cross", "cube", (4000, 4000, 80000, 80000), True, 43),
+    "sphere_fields": ("auto", "sphere", (4000, 80000), True, 44),
+    "sphere_cross": ("cross", "sphere", (4000, 4000, 80000, 80000), True, 45),
+}
+ALLTYPES_FIELDS = 8
+
+
+def alltypes_inputs(case):
+    """Seeded inputs of one case, shaped like test/test_alltypes.py's
+    (testing.random_cube / random_sphere: unit cube, or the whole sky uniform
+    in RA and sin DEC; fields are eight slices in x or in RA).  Returns the
+    catalogs as ("xyz", points) or ("radec", (ra, dec)), their fields (or
+    None), and the radii the reference's driver would pass to the counts
+    (for the sky, chords of the angles in degrees, as angular.py:40 does)."""
+    _, geom, sizes, with_fields, seed = ALLTYPES_CASES[case]
+    rs = np.random.RandomState(seed)
+    cats, fields = [], []
+    for n in sizes:
+        if geom == "cube":
+            p = rs.rand(n, 3)
+            cats.append(("xyz", p))
+            fields.append((p[:, 0] * ALLTYPES_FIELDS).astype("int32") if with_fields else None)
+        else:
+            ra = rs.rand(n) * 360.0
+            dec = np.arcsin(rs.rand(n) * 2.0 - 1.0) * 180.0 / np.pi
+            cats.append(("radec", (ra, dec)))
+            fields.append((ra / 360.0 * ALLTYPES_FIELDS).astype("int32") if with_fields else None)
+    if geom == "cube":
+        nominal = np.logspace(-2.5, -1.0, 6)
+        radii = nominal
+    else:
+        nominal = np.logspace(-1.5, 0.5, 6)
+        radii = 2.0 * np.sin(nominal * (np.pi / 180.0) / 2.0)
+    return cats, fields, nominal, radii
+
+
+def _sha1(*arrays):
+    h = hashlib.sha1()
+    for a in arrays:
+        if a is not None:
+            h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+def _fake_tree_sized(points, fields, n_fields, unique_size):
+    """The reference tree's attributes that the results classes read
+    (clustering.py:295-335): without fields, field_sizes is the unique size."""
+    if fields is None:
+        return types.SimpleNamespace(N_fields=1, field_sizes=np.array(unique_size),
+                                     points=points, fields=None)
+    return _fake_tree(points, fields, n_fields)
+
+
+def make_alltypes_goldens(R, ref_root):
+    clustering = _ref_python(ref_root)
+    out = {}
+    for case, (kind, geom, sizes, with_fields, seed) in ALLTYPES_CASES.items():
+        cats, fields, nominal, radii = alltypes_inputs(case)
+        pts = [c[1] if c[0] == "xyz" else R.radec2cart64(*c[1]) for c in cats]
+        nf = ALLTYPES_FIELDS if with_fields else 1
+        trs = [R.build(p, f, nf) for p, f in zip(pts, fields)]
+        fakes = [_fake_tree_sized(p, f, nf, t.size) for p, f, t in zip(pts, fields, trs)]
+        out[f"{case}/inputs_sha1"] = np.array(_sha1(*pts, *fields))
+        if kind == "auto":
+            d, r = 0, 1
+            arrays = {"dd": _binned(R, trs[d], pts[d], fields[d], nf, radii),
+                      "dr": _binned(R, trs[r], pts[d], fields[d], nf, radii),
+                      "rr": _binned(R, trs[r], pts[r], fields[r], nf, radii)}
+            res = clustering.autocorr_results(arrays["dd"], arrays["dr"], arrays["rr"],
+                                              fakes[d], fakes[r], clustering.est_landy_szalay,
+                                              radii)
+        else:
+            d1, d2, r1, r2 = range(4)
+            sz = [t.size for t in trs]
+            a, b = (d1, d2) if sz[d1] > sz[d2] else (d2, d1)
+            arrays = {"d1d2": _binned(R, trs[a], pts[b], fields[b], nf, radii),
+                      "d1r2": _binned(R, trs[r2], pts[d1], fields[d1], nf, radii),
+                      "d2r1": _binned(R, trs[r1], pts[d2], fields[d2], nf, radii)}
+            a, b = (r1, r2) if sz[r1] > sz[r2] else (r2, r1)
+            arrays["r1r2"] = _binned(R, trs[a], pts[b], fields[b], nf, radii)
+            res = clustering.crosscorr_results(arrays["d1d2"], arrays["d1r2"], arrays["d2r1"],
+                                               arrays["r1r2"], *fakes,
+                                               clustering.est_landy_szalay, radii)
+        for k, v in arrays.items():
+            out[f"{case}/{k}"] = v
+        # what twopoint.threedim / twopoint.angular set on the results
+        res.radii_nominal = res.radii_euclidean if geom == "cube" else nominal
+        res.radii_units = "Data units" if geom == "cube" else "degrees"
+        for est in ALLTYPES_ESTIMATORS:
+            res.estimator = getattr(clustering, "est_" + est.replace("-", "_"))
+            out[f"{case}/xi/{est}"] = res.estimate()
+            for err in ALLTYPES_ERRORS if with_fields else (None, "poisson"):
+                if err is not None:
+                    np.random.seed(11)
+                    out[f"{case}/err/{est}/{err}"] = res.error(err)
+                res.error_type = err
+                np.random.seed(11)
+                out[f"{case}/table/{est}/{err}"] = np.array(str(res))
+            if with_fields:
+                out[f"{case}/cov_jackknife/{est}"] = res.covariance("jackknife")
+                out[f"{case}/cov_ftf/{est}"] = res.covariance("ftf")
+        for t in trs:
+            R.destroy(t)
+    np.savez_compressed(os.path.join(HERE, "alltypes.npz"), **out)
 
 
 def make_coord_goldens(R):
