@@ -103,6 +103,25 @@ def test_far_from_origin(offset):
         N.destroy(t)
 
 
+def test_every_point_three_times():
+    """The reference's test/test_duplicates.py shape: 30,000 points each
+    repeated three times build a tree of 30,000 unique points (weight 3 each,
+    kdbuild.c:472-511); counts of a query sample equal the oracle's."""
+    from corruscant_b200 import clustering
+    rs = np.random.RandomState(47)
+    X = np.repeat(rs.rand(30000, 3), 3, axis=0)
+    f = (X[:, 0] * 4).astype(np.int32)
+    t = clustering.tree(X, f)
+    assert t.size == 30000 and t.N_fields == 4
+    assert np.array_equal(t.field_sizes, np.bincount(f, minlength=4))
+    idx = np.sort(rs.choice(len(X), 500, replace=False))
+    radii = np.array([0.0, 0.005, 0.02, 0.06])
+    got = N.count_points(t.ctree, X[idx], f[idx], 4, radii)
+    want = O.OracleTree(X, f, 4).brute_counts(X[idx], f[idx], 4, radii, nthreads=8)
+    assert np.array_equal(got, want)
+    assert np.all(got[1:].sum(axis=1) >= 3 * len(idx))  # each query meets its 3 copies
+
+
 def test_fields_above_255_follow_the_reference():
     """The tree side keeps the low 8 bits of a field id (kdtree.h field:8), the
     query side the full id; an autocorrelation with such fields is counted the
