@@ -253,42 +253,50 @@ def make_estimator_goldens(R, ref_root):
 ALLTYPES_ESTIMATORS = ("standard", "hamilton", "landy-szalay")
 ALLTYPES_ERRORS = (None, "poisson", "ftf", "jackknife", "bootstrap")
 ALLTYPES_CASES = {
-    # name: (auto | cross, cube | sphere, catalog sizes, eight fields?, seed)
-    "cube_nofield": ("auto", "cube", (4000, 80000), False, 41),
-    "cube_fields": ("auto", "cube", (4000, 80000), True, 42),
-    "cube_cross": ("cross", "cube", (4000, 4000, 80000, 80000), True, 43),
-    "sphere_fields": ("auto", "sphere", (4000, 80000), True, 44),
-    "sphere_cross": ("cross", "sphere", (4000, 4000, 80000, 80000), True, 45),
+    # test/test_alltypes.py: 4k data, 20x randoms, eight fields (or none),
+    # edges logspace(-2.5, -1, 6) in the cube, logspace(-1.5, 0.5, 6) degrees
+    # on the sky
+    "cube_nofield": dict(kind="auto", geom="cube", sizes=(4000, 80000), nfields=0, seed=41,
+                         edges=(-2.5, -1.0)),
+    "cube_fields": dict(kind="auto", geom="cube", sizes=(4000, 80000), nfields=8, seed=42,
+                        edges=(-2.5, -1.0)),
+    "cube_cross": dict(kind="cross", geom="cube", sizes=(4000, 4000, 80000, 80000), nfields=8,
+                       seed=43, edges=(-2.5, -1.0)),
+    "sphere_fields": dict(kind="auto", geom="sphere", sizes=(4000, 80000), nfields=8, seed=44,
+                          edges=(-1.5, 0.5)),
+    "sphere_cross": dict(kind="cross", geom="sphere", sizes=(4000, 4000, 80000, 80000),
+                         nfields=8, seed=45, edges=(-1.5, 0.5)),
+    # test/angular.py: 10k data, 200k randoms on the sky, RA quadrants as
+    # fields, edges logspace(-2, 0, 6) degrees
+    "sphere_quadrants": dict(kind="auto", geom="sphere", sizes=(10000, 200000), nfields=4,
+                             seed=46, edges=(-2.0, 0.0)),
 }
-ALLTYPES_FIELDS = 8
 
 
 def alltypes_inputs(case):
-    """Seeded inputs of one case, shaped like test/test_alltypes.py's
+    """Seeded inputs of one case, shaped like the reference's test scripts
     (testing.random_cube / random_sphere: unit cube, or the whole sky uniform
-    in RA and sin DEC; fields are eight slices in x or in RA).  Returns the
+    in RA and sin DEC; fields are equal slices in x or in RA).  Returns the
     catalogs as ("xyz", points) or ("radec", (ra, dec)), their fields (or
-    None), and the radii the reference's driver would pass to the counts
-    (for the sky, chords of the angles in degrees, as angular.py:40 does)."""
-    _, geom, sizes, with_fields, seed = ALLTYPES_CASES[case]
-    rs = np.random.RandomState(seed)
+    None), the nominal edges and the radii the reference's driver would pass
+    to the counts (for the sky, chords of the angles in degrees, as
+    angular.py:40 does)."""
+    c = ALLTYPES_CASES[case]
+    geom, nf = c["geom"], c["nfields"]
+    rs = np.random.RandomState(c["seed"])
     cats, fields = [], []
-    for n in sizes:
+    for n in c["sizes"]:
         if geom == "cube":
             p = rs.rand(n, 3)
             cats.append(("xyz", p))
-            fields.append((p[:, 0] * ALLTYPES_FIELDS).astype("int32") if with_fields else None)
+            fields.append((p[:, 0] * nf).astype("int32") if nf else None)
         else:
             ra = rs.rand(n) * 360.0
             dec = np.arcsin(rs.rand(n) * 2.0 - 1.0) * 180.0 / np.pi
             cats.append(("radec", (ra, dec)))
-            fields.append((ra / 360.0 * ALLTYPES_FIELDS).astype("int32") if with_fields else None)
-    if geom == "cube":
-        nominal = np.logspace(-2.5, -1.0, 6)
-        radii = nominal
-    else:
-        nominal = np.logspace(-1.5, 0.5, 6)
-        radii = 2.0 * np.sin(nominal * (np.pi / 180.0) / 2.0)
+            fields.append((ra / 360.0 * nf).astype("int32") if nf else None)
+    nominal = np.logspace(c["edges"][0], c["edges"][1], 6)
+    radii = nominal if geom == "cube" else 2.0 * np.sin(nominal * (np.pi / 180.0) / 2.0)
     return cats, fields, nominal, radii
 
 
@@ -312,10 +320,11 @@ def _fake_tree_sized(points, fields, n_fields, unique_size):
 def make_alltypes_goldens(R, ref_root):
     clustering = _ref_python(ref_root)
     out = {}
-    for case, (kind, geom, sizes, with_fields, seed) in ALLTYPES_CASES.items():
+    for case, c in ALLTYPES_CASES.items():
+        kind, geom, with_fields = c["kind"], c["geom"], c["nfields"] > 0
         cats, fields, nominal, radii = alltypes_inputs(case)
-        pts = [c[1] if c[0] == "xyz" else R.radec2cart64(*c[1]) for c in cats]
-        nf = ALLTYPES_FIELDS if with_fields else 1
+        pts = [x[1] if x[0] == "xyz" else R.radec2cart64(*x[1]) for x in cats]
+        nf = c["nfields"] if with_fields else 1
         trs = [R.build(p, f, nf) for p, f in zip(pts, fields)]
         fakes = [_fake_tree_sized(p, f, nf, t.size) for p, f, t in zip(pts, fields, trs)]
         out[f"{case}/inputs_sha1"] = np.array(_sha1(*pts, *fields))

@@ -1,6 +1,7 @@
-"""The reference's test/test_alltypes.py workloads: 3-D and angular, auto and
-cross, with and without fields (tests/golden/alltypes.npz, made by
-tests/golden/make_golden.py from the reference itself).
+"""The workloads of the reference's test/test_alltypes.py (3-D and angular,
+auto and cross, with and without fields) and test/angular.py (10k / 200k
+points on the sky, RA quadrants as fields): tests/golden/alltypes.npz, made
+by tests/golden/make_golden.py from the reference itself.
 
 On the CPU, the results classes fed the reference's counts give every
 estimator x error type, the covariances and the printed results tables bit
@@ -44,7 +45,7 @@ def _points(cats):
 
 def _check_values(g, case, res):
     """Every estimator x error type, covariance and table against the golden."""
-    with_fields = MG.ALLTYPES_CASES[case][3]
+    with_fields = MG.ALLTYPES_CASES[case]["nfields"] > 0
     for est in MG.ALLTYPES_ESTIMATORS:
         res.estimator = clustering._estimator(est)
         assert np.array_equal(_bits(res.estimate()), _bits(g[f"{case}/xi/{est}"])), est
@@ -67,24 +68,23 @@ def _check_values(g, case, res):
                 res.error(err)
 
 
-def _fake_tree(points, fields):
+def _fake_tree(points, fields, nf):
     """The tree attributes the results classes read; without fields the
     field size is the unique size (all points are distinct here)."""
     if fields is None:
         return types.SimpleNamespace(N_fields=1, field_sizes=np.array(len(points)))
-    return types.SimpleNamespace(
-        N_fields=MG.ALLTYPES_FIELDS,
-        field_sizes=np.bincount(fields, minlength=MG.ALLTYPES_FIELDS))
+    return types.SimpleNamespace(N_fields=nf, field_sizes=np.bincount(fields, minlength=nf))
 
 
 @pytest.mark.parametrize("case", CASES)
 def test_alltypes_estimators_from_reference_counts(golden, case):
     g = golden("alltypes.npz")
-    kind, geom, _, _, _ = MG.ALLTYPES_CASES[case]
+    c = MG.ALLTYPES_CASES[case]
+    kind, geom = c["kind"], c["geom"]
     cats, fields, nominal, radii = MG.alltypes_inputs(case)
     pts = _points(cats)
     assert MG._sha1(*pts, *fields) == str(g[f"{case}/inputs_sha1"])
-    fakes = [_fake_tree(p, f) for p, f in zip(pts, fields)]
+    fakes = [_fake_tree(p, f, c["nfields"]) for p, f in zip(pts, fields)]
     arrays = [g[f"{case}/{k}"] for k in _names(kind)]
     est = clustering.est_landy_szalay
     if kind == "auto":
@@ -100,7 +100,8 @@ def test_alltypes_estimators_from_reference_counts(golden, case):
 @pytest.mark.parametrize("case", CASES)
 def test_alltypes_case_through_the_api(golden, case):
     g = golden("alltypes.npz")
-    kind, geom, _, _, _ = MG.ALLTYPES_CASES[case]
+    c = MG.ALLTYPES_CASES[case]
+    kind, geom = c["kind"], c["geom"]
     cats, fields, nominal, radii = MG.alltypes_inputs(case)
     pts = _points(cats)
     # the reference's inputs (for the sky, our conversion gives the
