@@ -35,3 +35,16 @@ def golden_sets(npz):
 
 def none_if_empty(a):
     return None if a.size == 0 else a.astype(np.int32)
+
+
+def verify_heap(nodes):
+    """The reference's verify_tree rule (kdtest.c:73-99) over a whole node
+    array: a left child's coordinate in its parent's split dimension is <=
+    the parent's, a right child's is >=."""
+    dim = nodes["dim"].astype(np.int64)
+    xyz = nodes["xyz"]
+    par = np.arange(1, len(dim) // 2)
+    left = par[nodes["has_l"][par] != 0]
+    right = par[nodes["has_r"][par] != 0]
+    assert np.all(xyz[2 * left, dim[left]] <= xyz[left, dim[left]])
+    assert np.all(xyz[2 * right + 1, dim[right]] >= xyz[right, dim[right]])

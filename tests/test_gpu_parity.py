@@ -7,7 +7,7 @@ FP32 + FP64-recheck mode and the plain FP64 mode.
 import numpy as np
 import pytest
 
-from conftest import golden_sets, none_if_empty
+from conftest import golden_sets, none_if_empty, verify_heap
 from corruscant_b200 import _native as N
 from oracle import oracle as O
 
@@ -47,6 +47,40 @@ def test_permutation_matches_oracle(golden):
             assert np.array_equal(N.permutation(t), ot.inorder()), name
         finally:
             N.destroy(t)
+
+
+def _large_set(kind):
+    rs = np.random.RandomState(48)
+    if kind == "clustered_1M":
+        # the clustered workload's data catalog: Neyman-Scott, 10,000 parents
+        parents = rs.rand(10000, 3)
+        p = (np.repeat(parents, 100, axis=0) + rs.normal(0.0, 0.005, (1_000_000, 3))) % 1.0
+        f = (16 * np.floor(4 * p[:, 0]) + 4 * np.floor(4 * p[:, 1]) +
+             np.floor(4 * p[:, 2])).astype(np.int32)
+        return p, f, 64
+    # a 1/64 lattice: ties in every coordinate, about half the rows repeated
+    p = rs.randint(0, 64, (400_000, 3)) / 64.0
+    return p, (p[:, 0] * 3).astype(np.int32), 3
+
+
+@pytest.mark.parametrize("kind", ["clustered_1M", "lattice_400k"])
+def test_large_trees_match_the_oracle_node_for_node(kind):
+    """Bit-exact node array and in-order permutation at the sizes the
+    benchmarks build (the small sets are pinned to the reference itself; the
+    oracle is pinned to it on those and on random lattice and clustered sets)."""
+    p, f, nf = _large_set(kind)
+    t = _tree(p, f, nf)
+    try:
+        ot = O.OracleTree(p, f, nf)
+        assert t.size == ot.size and t.memsize == ot.memsize
+        nodes, want = N.node_fields(t), ot.nodes()
+        assert np.array_equal(nodes["xyz"].view(np.int64), want["xyz"].view(np.int64))
+        for k in ("field", "weight", "has_l", "has_r", "dim"):
+            assert np.array_equal(nodes[k], want[k]), k
+        assert np.array_equal(N.permutation(t), ot.inorder())
+        verify_heap(nodes)
+    finally:
+        N.destroy(t)
 
 
 def test_pair_count_matches_reference_goldens(golden):

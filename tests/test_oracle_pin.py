@@ -11,7 +11,7 @@
 import numpy as np
 import pytest
 
-from conftest import golden_sets, none_if_empty
+from conftest import golden_sets, none_if_empty, verify_heap
 from oracle import oracle as O
 
 
@@ -129,3 +129,22 @@ def test_oracle_matches_live_reference_random():
         for r in (0.0, 0.01, 0.07, 0.3):
             assert np.array_equal(R.pair_count(rt, q, qf, nf, r), ot.pair_count(q, qf, nf, r))
         R.destroy(rt)
+
+
+def test_heap_rule_holds_and_catches_a_planted_violation(golden):
+    """The reference's verify_tree rule holds on oracle trees (golden sets
+    and a 200k lattice with ties), and fails once a child is moved to the
+    wrong side of its parent (the mistake is planted in the oracle's nodes)."""
+    rs = np.random.RandomState(49)
+    p = rs.randint(0, 32, (200_000, 3)) / 32.0
+    nodes = O.OracleTree(p, (p[:, 1] * 2).astype(np.int32), 2).nodes()
+    verify_heap(nodes)
+    for name, s in golden_sets(golden("trees.npz")).items():
+        f = none_if_empty(s["fields"])
+        verify_heap(O.OracleTree(s["points"], f, int(s["num_fields"])).nodes())
+    bad = {k: v.copy() for k, v in nodes.items()}
+    i = int(np.nonzero(bad["has_l"][1:len(bad["dim"]) // 2])[0][100]) + 1
+    d = int(bad["dim"][i])
+    bad["xyz"][2 * i, d] = bad["xyz"][i, d] + 1.0
+    with pytest.raises(AssertionError):
+        verify_heap(bad)
