@@ -90,6 +90,10 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
         kd_set_error(KD_EINVAL, "tree_construct: need at least one point");
         return t;
     }
+    if (length > KD_MAX_POINTS) {
+        kd_set_error(KD_EINVAL, "tree_construct: %d points, at most %d", length, KD_MAX_POINTS);
+        return t;
+    }
     h = (kd_handle *)calloc(1, sizeof *h);
     if (!h) {
         kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
@@ -360,12 +364,19 @@ int kd_count_points(kdtree_t tree, const double *xyz, const int *fields, int len
     clear_error();
     h = lookup_or_fail(&tree, "kd_count_points");
     if (!h) return KD_EINVAL;
-    if (length < 0 || nradii < 0 || (length > 0 && !xyz)) {
+    if (length < 0 || length > KD_MAX_POINTS || nradii < 0 || (length > 0 && !xyz) ||
+        (nradii > 0 && (!radii || !out))) {
         kd_set_error(KD_EINVAL, "kd_count_points: bad arguments");
         return KD_EINVAL;
     }
+    if (num_fields < 1 || tree.num_fields < 1) {
+        kd_set_error(KD_EFIELD, "field counts must be positive");
+        return KD_EFIELD;
+    }
     if (length == 0) {
-        memset(out, 0, sizeof(long long) * (size_t)num_fields * tree.num_fields * nradii);
+        if (nradii > 0)
+            memset(out, 0, sizeof(long long) * (size_t)num_fields * (size_t)tree.num_fields *
+                               (size_t)nradii);
         if (stats) memset(stats, 0, sizeof *stats);
         return KD_OK;
     }
@@ -373,7 +384,9 @@ int kd_count_points(kdtree_t tree, const double *xyz, const int *fields, int len
     rc = query_catalog(xyz, fields, length, num_fields, &qc, &empty);
     if (rc != KD_OK) return rc;
     if (empty) {
-        memset(out, 0, sizeof(long long) * (size_t)num_fields * tree.num_fields * nradii);
+        if (nradii > 0)
+            memset(out, 0, sizeof(long long) * (size_t)num_fields * (size_t)tree.num_fields *
+                               (size_t)nradii);
         if (stats) memset(stats, 0, sizeof *stats);
         return KD_OK;
     }
@@ -394,6 +407,10 @@ int kd_count_radii_shard(kdtree_t tree, kdtree_t query, const double *radii, int
     if (!hq) return KD_EINVAL;
     if (nshards < 1 || shard < 0 || shard >= nshards) {
         kd_set_error(KD_EINVAL, "kd_count_radii_shard: shard %d of %d", shard, nshards);
+        return KD_EINVAL;
+    }
+    if (nradii < 0 || (nradii > 0 && (!radii || !out))) {
+        kd_set_error(KD_EINVAL, "kd_count_radii: bad radius count or NULL array");
         return KD_EINVAL;
     }
     return count_catalogs(&ht->cat, tree.num_fields, &hq->cat, query.num_fields, radii, nradii,

@@ -37,17 +37,8 @@ extern "C" {
 #define KD_LEAF_TARGET 64  /* unique points per counting leaf, upper bound */
 #define KD_MAX_EDGES 64    /* distinct finite squared edges per count job */
 
-/* status codes (negative), shared by host and device error words */
-#define KD_OK 0
-#define KD_EINVAL -1
-#define KD_ENOMEM -2
-#define KD_EDUP -3        /* >= 256 copies of one point (weight:8 would wrap) */
-#define KD_ENAN -4        /* NaN coordinate in a tree */
-#define KD_EFIELD -5      /* field ids overflow the reference counter layout */
-#define KD_ECUDA -6
-#define KD_ENODEV -7      /* no usable CUDA device / extension not usable */
-#define KD_EINTERNAL -8   /* a device-side bound was hit (stack, sizes) */
-#define KD_ERADIUS -9     /* negative radius (the reference prune is not defined) */
+/* the status codes (KD_OK, KD_EINVAL, ...) and KD_MAX_POINTS are public:
+ * include/kdtree.h; the device error words use the same codes */
 
 typedef struct kd_catalog {
     int device;

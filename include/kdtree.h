@@ -93,6 +93,24 @@ void destroy(kdtree_t tree);
 #define KD_MODE_MIXED 0 /* FP32 distances + FP64 recheck near edges (default) */
 #define KD_MODE_FP64 1  /* every distance in FP64 */
 
+/* Status codes: 0 or negative.  Where the reference prints and exits
+ * (kdbuild.c:73-79, :234-239, :508-511; kdquery.c:176-179) these calls
+ * return a code, and kd_last_error() holds the message. */
+#define KD_OK 0
+#define KD_EINVAL -1      /* bad argument: count, pointer, mode, shard, handle */
+#define KD_ENOMEM -2      /* host or device memory exhausted */
+#define KD_EDUP -3        /* >= 256 copies of one point (weight:8 would wrap) */
+#define KD_ENAN -4        /* NaN coordinate in a tree */
+#define KD_EFIELD -5      /* field counts or ids do not fit the qfield*Fq + tfield counter */
+#define KD_ECUDA -6       /* a CUDA call failed */
+#define KD_ENODEV -7      /* no usable CUDA device */
+#define KD_EINTERNAL -8   /* a device-side bound was hit (stack, sizes) */
+#define KD_ERADIUS -9     /* negative radius (the reference's pruning is not defined there) */
+
+/* Largest catalog, raw points (duplicates included): the node heap of
+ * 2^(floor(log2 n) + 1) entries is indexed by int, as in the reference. */
+#define KD_MAX_POINTS 1073741823
+
 typedef struct kd_count_stats {
     long long pairs_tested;    /* distances evaluated in tiles */
     long long pairs_rechecked; /* pairs recomputed in FP64 after an FP32 band hit */

@@ -231,6 +231,36 @@ static void scenario_faults(void)
         CHECK(kd_count_radii(t, t, r, 64, 0, o65, NULL) == 0, "64 distinct radii refused");
         CHECK(kd_count_radii(t, t, (const double[]){0.1, -0.1}, 2, 0, o65, NULL) < 0, "neg");
     }
+    /* malformed counts and pointers are errors, never memory accesses */
+    CHECK(kd_count_radii(t, t, RADII, -1, 0, out, NULL) == KD_EINVAL, "negative radius count");
+    CHECK(kd_count_radii(t, t, NULL, 3, 0, out, NULL) == KD_EINVAL, "NULL radii");
+    CHECK(kd_count_radii(t, t, RADII, NR, 0, NULL, NULL) == KD_EINVAL, "NULL output");
+    CHECK(kd_count_batch(&t, &t, 1, RADII, -3, 0, out, NULL) == KD_EINVAL, "batch: negative count");
+    CHECK(kd_count_points(t, a.xyz, a.f, 0, 0, RADII, NR, 0, out, NULL) == KD_EFIELD,
+          "no queries, zero query fields");
+    CHECK(kd_count_points(t, a.xyz, a.f, 0, -4, RADII, NR, 0, out, NULL) == KD_EFIELD,
+          "no queries, negative query fields");
+    CHECK(kd_count_points(t, a.xyz, a.f, 0, a.nf, RADII, NR, 0, NULL, NULL) == KD_EINVAL,
+          "no queries, NULL output");
+    CHECK(kd_count_points(t, a.xyz, a.f, 0, a.nf, NULL, NR, 0, out, NULL) == KD_EINVAL,
+          "no queries, NULL radii");
+    {
+        double nanq[6] = {NAN, 0.1, 0.2, 0.3, NAN, 0.5};
+        CHECK(kd_count_points(t, nanq, NULL, 2, 0, RADII, NR, 0, out, NULL) == KD_EFIELD,
+              "NaN-only queries, zero query fields");
+        CHECK(kd_count_points(t, nanq, NULL, 2, 1, RADII, 0, 0, NULL, NULL) == KD_OK,
+              "no radii, no output array");
+    }
+    {
+        /* the size check comes before any point is read (a.xyz holds 150) */
+        kdtree_t big = tree_construct(a.xyz, a.f, KD_MAX_POINTS + 1, a.nf);
+        CHECK(!big.node_data && kd_last_error(msg, sizeof msg) == KD_EINVAL &&
+                  strstr(msg, "at most"), "2^30 points: %s", msg);
+        CHECK(kd_count_points(t, a.xyz, a.f, KD_MAX_POINTS + 1, a.nf, RADII, NR, 0, out, NULL) ==
+                  KD_EINVAL, "2^30 query points");
+        CHECK(pair_count(t, a.xyz, a.f, KD_MAX_POINTS + 1, a.nf, 0.1, 1) == NULL,
+              "pair_count with 2^30 points");
+    }
     destroy(t);
 
     /* injected device-layer failures: clean errors, nothing leaks */
