@@ -263,3 +263,11 @@ class RefLib:
         out = np.empty((ra.size, 3))
         self.co.radecdist2cart64(_dp(ra), _dp(dec), _dp(dist), _dp(out), c_int(ra.size))
         return out
+
+    def radec2sph64(self, ra, dec):
+        """The reference's coordmath.c:73-80: (theta, phi) in radians."""
+        ra = np.require(ra, dtype=np.float64, requirements="AC")
+        dec = np.require(dec, dtype=np.float64, requirements="AC")
+        theta, phi = np.empty(ra.size), np.empty(ra.size)
+        self.co.radec2sph64(_dp(ra), _dp(dec), _dp(theta), _dp(phi), c_int(ra.size))
+        return theta, phi

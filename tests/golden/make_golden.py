@@ -17,7 +17,7 @@ Outputs (all small):
                    (numpy seed 3, 6 edges logspace(-2.5,-1), fields floor(4x)):
                    DD/DR/RR per bin and the reference estimator / error values
   cross.npz        a small cross-correlation with the reference's estimators
-  coords.npz       reference radec2cart64 / radecdist2cart64 outputs
+  coords.npz       reference radec2cart64 / radecdist2cart64 / radec2sph64 outputs
   alltypes.npz     the workloads of the reference's test/test_alltypes.py
                    (3-D and angular, auto and cross, with and without
                    fields; seeded inputs): counts, every estimator x error
@@ -382,8 +382,10 @@ def make_coord_goldens(R):
     ra = np.concatenate([ra, special, rs.rand(16) * 90])
     dec = np.concatenate([dec, rs.rand(16) * 180 - 90, special.clip(-90, 90)])
     dist = rs.rand(ra.size) * 3000.0
+    theta, phi = R.radec2sph64(ra, dec)
     np.savez_compressed(os.path.join(HERE, "coords.npz"), ra=ra, dec=dec, dist=dist,
-                        xyz=R.radec2cart64(ra, dec), xyzd=R.radecdist2cart64(ra, dec, dist))
+                        xyz=R.radec2cart64(ra, dec), xyzd=R.radecdist2cart64(ra, dec, dist),
+                        theta=theta, phi=phi)
 
 
 if __name__ == "__main__":

@@ -147,6 +147,36 @@ def test_coordinates_bit_identical_to_reference(golden):
     _assert_bits(twopoint.threedim.cartesian(c["ra"], c["dec"], c["dist"]), c["xyzd"])
 
 
+def test_spherical_coordinates_bit_identical_to_reference(golden):
+    """radec2sph64 (coordmath.c:73-80) of libcoords.so."""
+    c = golden("coords.npz")
+    ra = np.require(c["ra"], dtype=np.float64, requirements="AC")
+    dec = np.require(c["dec"], dtype=np.float64, requirements="AC")
+    theta, phi = np.empty(ra.size), np.empty(ra.size)
+    _native.coordlib().radec2sph64(_native.dptr(ra), _native.dptr(dec), _native.dptr(theta),
+                                   _native.dptr(phi), ra.size)
+    _assert_bits(theta, c["theta"])
+    _assert_bits(phi, c["phi"])
+
+
+def test_cartesian_from_redshift_and_cosmology():
+    """threedim.cartesian with z and a cosmology object (anything with
+    comoving_distance, as astropy's; threedim.py:78-81) equals the call with
+    those distances."""
+    class Cosmology:
+        def comoving_distance(self, z):
+            return 2997.92458 * z / (1.0 + 0.3 * z)
+
+    rs = np.random.RandomState(50)
+    ra, dec, z = rs.rand(500) * 360, rs.rand(500) * 180 - 90, rs.rand(500) * 2
+    _assert_bits(twopoint.threedim.cartesian(ra, dec, z=list(z), cosmology=Cosmology()),
+                 twopoint.threedim.cartesian(ra, dec, Cosmology().comoving_distance(z)))
+    # a given distance takes precedence over a redshift
+    d = rs.rand(500) * 100
+    _assert_bits(twopoint.threedim.cartesian(ra, dec, d, z=z, cosmology=Cosmology()),
+                 twopoint.threedim.cartesian(ra, dec, d))
+
+
 def test_chord_edges_are_the_reference_expression():
     deg = np.logspace(-3, np.log10(2.0), 16)
     _assert_bits(twopoint.angular.chord(deg), 2. * np.sin(deg * (np.pi / 180.) / 2.))

@@ -98,6 +98,9 @@ def test_coords_match_reference_goldens(golden):
     assert np.array_equal(xyz.view(np.int64), c["xyz"].view(np.int64))
     xyzd = O.radecdist2cart64(c["ra"], c["dec"], c["dist"])
     assert np.array_equal(xyzd.view(np.int64), c["xyzd"].view(np.int64))
+    theta, phi = O.radec2sph64(c["ra"], c["dec"])
+    assert np.array_equal(theta.view(np.int64), c["theta"].view(np.int64))
+    assert np.array_equal(phi.view(np.int64), c["phi"].view(np.int64))
 
 
 def test_weight_overflow_is_an_error():
