@@ -33,6 +33,20 @@ __all__ = ["tree", "validate_points", "validate_fields", "est_standard", "est_ha
 #: (default) or every distance in FP64; both give identical counts
 DEFAULT_MODE = _native.KD_MODE_MIXED
 
+#: the C ABI's structures under the reference's ctypes names
+#: (clustering.py:30-45; ``kdtree`` is the full 64-byte kdtree_t)
+datum = _native.Datum
+node = _native.Node
+kdtree = _native.KdTree
+
+
+def __getattr__(name):
+    """``kdlib``: the loaded libkdtree (clustering.py:47-71), opened on first
+    access."""
+    if name == "kdlib":
+        return _native.kdlib()
+    raise AttributeError(name)
+
 
 def validate_points(points):
     """(N,3) C-contiguous float array of points; a (3,N) array is transposed
@@ -134,12 +148,21 @@ class tree:
                 raise ValueError("At least two unique field IDs must be provided if using "
                                  "error fields")
             self.fields = fields
-            self.field_sizes = np.bincount(fields, minlength=self.N_fields)
+            self.field_sizes = self._calc_field_sizes()
         self.points = np.require(points, dtype="float64", requirements="AC")
-        self.ctree = _native.build_tree(self.points, self.fields, self.N_fields)
+        self._make_tree()
         self.size = self.ctree.size
         if fields is None:
             self.field_sizes = np.array(self.size)
+
+    def _calc_field_sizes(self):
+        """Points per field id 0 .. N_fields - 1 (clustering.py:336-338)."""
+        return np.bincount(self.fields, minlength=self.N_fields)
+
+    def _make_tree(self):
+        """Build the GPU tree of ``points`` / ``fields`` into ``ctree``
+        (clustering.py:340-349)."""
+        self.ctree = _native.build_tree(self.points, self.fields, self.N_fields)
 
     def __del__(self):
         ct = getattr(self, "ctree", None)

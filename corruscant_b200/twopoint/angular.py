@@ -10,6 +10,14 @@ from .. import _native, clustering
 __all__ = ["autocorr", "crosscorr", "cartesian", "chord"]
 
 
+def __getattr__(name):
+    """``coordlib``: the loaded libcoords, as the reference module binds it
+    (angular.py:27-35), opened on first access."""
+    if name == "coordlib":
+        return _native.coordlib()
+    raise AttributeError(name)
+
+
 def chord(radii_deg):
     """Chord length of angular separations given in degrees."""
     radii_deg = np.array(radii_deg)

@@ -9,6 +9,14 @@ from .. import _native, clustering
 __all__ = ["autocorr", "crosscorr", "cartesian"]
 
 
+def __getattr__(name):
+    """``coordlib``: the loaded libcoords, as the reference module binds it
+    (threedim.py:28-37), opened on first access."""
+    if name == "coordlib":
+        return _native.coordlib()
+    raise AttributeError(name)
+
+
 def autocorr(data_tree, rand_tree, radii, **kwargs):
     """DD/DR/RR estimator results for bin edges ``radii`` (threedim.py:39-46)."""
     res = clustering._autocorr(data_tree, rand_tree, radii, **kwargs)

@@ -177,6 +177,43 @@ def test_cartesian_from_redshift_and_cosmology():
                  twopoint.threedim.cartesian(ra, dec, d))
 
 
+# every public name of the reference package (corruscant/__init__.py,
+# clustering.py, twopoint/angular.py, twopoint/threedim.py) and the methods
+# of its classes
+REFERENCE_API = {
+    "": ["PROJECT_PATH", "loadlib", "kdlib", "coordlib", "clustering", "twopoint"],
+    "clustering": ["node", "datum", "kdtree", "kdlib", "_query_tree", "validate_points",
+                   "validate_fields", "est_landy_szalay", "est_hamilton", "est_standard",
+                   "_autocorr", "_crosscorr", "tree", "results", "autocorr_results",
+                   "crosscorr_results"],
+    "twopoint.angular": ["coordlib", "autocorr", "crosscorr", "cartesian"],
+    "twopoint.threedim": ["coordlib", "autocorr", "crosscorr", "cartesian"],
+}
+REFERENCE_METHODS = {
+    "tree": ["_calc_field_sizes", "_make_tree", "__del__"],
+    "results": ["total_pair_counts", "ftf_pair_counts", "jackknife_pair_counts",
+                "bootstrap_pair_counts", "bootstrap_error", "jackknife_error", "ftf_error",
+                "poisson_error", "estimate", "covariance", "error", "__str__"],
+}
+
+
+def test_reference_api_names_exist():
+    import importlib
+    for mod, names in REFERENCE_API.items():
+        m = importlib.import_module("corruscant_b200" + ("." + mod if mod else ""))
+        for n in names:
+            assert getattr(m, n, None) is not None, (mod, n)
+    for cls, methods in REFERENCE_METHODS.items():
+        for n in methods:
+            assert callable(getattr(getattr(clustering, cls), n, None)), (cls, n)
+    import corruscant_b200
+    assert corruscant_b200.kdlib.tree_construct.restype is clustering.kdtree
+    assert ctypes.sizeof(clustering.kdtree) == 64 and ctypes.sizeof(clustering.node) == 40
+    assert corruscant_b200.coordlib is twopoint.angular.coordlib
+    with pytest.raises(AttributeError):
+        corruscant_b200.not_a_name
+
+
 def test_chord_edges_are_the_reference_expression():
     deg = np.logspace(-3, np.log10(2.0), 16)
     _assert_bits(twopoint.angular.chord(deg), 2. * np.sin(deg * (np.pi / 180.) / 2.))
