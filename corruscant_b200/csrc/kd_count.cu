@@ -35,6 +35,7 @@
 #include <exception>
 #include <new>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <cmath>
 #include <mutex>
@@ -1058,12 +1059,24 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
     // batches of global blocks whose tile records fit the buffer: up to 2^30
     // records (16 GiB) or a quarter of the free memory, so that on a B200 a
     // full DD + DR + RR batch of 20M-point catalogs runs as one launch
-    long long total = 0;
-    for (int i = 0; i < nb; i++) total += hcnt[i];
+    long long total = 0, maxblk = 0;
+    for (int i = 0; i < nb; i++) {
+        total += hcnt[i];
+        maxblk = std::max<long long>(maxblk, hcnt[i]);
+    }
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
     long long cap = std::max<long long>(
         1 << 20, std::min<long long>(1LL << 30, (long long)(freeb / 4 / sizeof(uint4))));
+    // KD_TILE_RECORD_CAP (records, > 0) lowers the batch size: it exercises
+    // the multi-batch path on small counts
+    if (const char *env = getenv("KD_TILE_RECORD_CAP")) {
+        const long long v = atoll(env);
+        if (v > 0) cap = v;
+    }
+    // every batch holds at least one whole block: the buffer must take the
+    // largest block's records (a failed allocation is reported, not overrun)
+    cap = std::max(cap, maxblk);
     cap = std::min<long long>(cap, std::max<long long>(total, 1));
     uint4 *rec = pool.alloc<uint4>(cap);
     long long *off = pool.alloc<long long>(nb + 1);

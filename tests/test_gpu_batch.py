@@ -4,6 +4,8 @@ Every job of a batch must give exactly what kd_count_radii gives for it
 alone (and, for the small ones, what the exhaustive oracle gives), whatever
 the mix of sizes, field counts and duplicates in the batch.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -136,6 +138,34 @@ def test_many_tiny_jobs_in_one_batch():
     finally:
         for t in trees:
             N.destroy(t)
+
+
+def test_counts_split_over_many_record_batches():
+    """With the tile-record buffer capped (KD_TILE_RECORD_CAP), a count runs
+    as many traversal + tile batches; the counts equal the single-batch
+    counts in both precisions, and every pair is still tested exactly once."""
+    rs = np.random.RandomState(25)
+    d, r = rs.rand(20000, 3), rs.rand(60000, 3)
+    td = N.build_tree(d, (d[:, 0] * 4).astype(np.int32), 4)
+    tr = N.build_tree(r, (r[:, 0] * 4).astype(np.int32), 4)
+    radii = np.logspace(-2.5, -1, 8)
+    jobs = [(td, td), (tr, td), (tr, tr)]
+    try:
+        want, s1 = N.count_batch(jobs, radii, with_stats=True)
+        assert s1["tile_launches"] == 1
+        os.environ["KD_TILE_RECORD_CAP"] = "3000"
+        try:
+            got, s2 = N.count_batch(jobs, radii, with_stats=True)
+            got64 = N.count_batch(jobs, radii, mode=N.KD_MODE_FP64)
+        finally:
+            del os.environ["KD_TILE_RECORD_CAP"]
+        assert s2["tile_launches"] > 10
+        assert s2["pairs_tested"] == s1["pairs_tested"] and s2["entries"] == s1["entries"]
+        for w, g, g64 in zip(want, got, got64):
+            assert np.array_equal(g, w) and np.array_equal(g64, w)
+    finally:
+        N.destroy(td)
+        N.destroy(tr)
 
 
 def test_batch_argument_errors():
