@@ -352,7 +352,10 @@ class Dist:
             import torch.distributed as dist
             if backend == "nccl":
                 torch.cuda.set_device(self.local)
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            # short: between collectives a rank works alone for seconds at
+            # most (tree builds; rank 0's GEMM peak measurement), so a rank
+            # that died ends the others' next collective with an error
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.dist, self.torch = dist, torch
 
     def barrier(self):
