@@ -352,10 +352,11 @@ class Dist:
             import torch.distributed as dist
             if backend == "nccl":
                 torch.cuda.set_device(self.local)
-            # short: between collectives a rank works alone for seconds at
-            # most (tree builds; rank 0's GEMM peak measurement), so a rank
-            # that died ends the others' next collective with an error
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            # short, so that a rank that died ends the others' next
+            # collective with an error; long enough for the slowest gap
+            # between collectives: every rank generating the 20M-point
+            # workload on shared host cores before the first one
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
             self.dist, self.torch = dist, torch
 
     def barrier(self):
