@@ -229,7 +229,7 @@ static int count_jobs(const kd_catalog *const *tcs, const int *Fts, const kd_cat
             kd_set_error(KD_ERADIUS, "negative radius %g", radii[k]);
             return KD_ERADIUS;
         }
-    memset(out, 0, sizeof(long long) * total);
+    if (total) memset(out, 0, sizeof(long long) * total);
     if (stats) memset(stats, 0, sizeof *stats);
     rsq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
     uniq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
@@ -308,6 +308,37 @@ static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, in
     return count_jobs(&tc, &Ft, &qc, &Fq, 1, radii, nradii, mode, shard, nshards, out, stats);
 }
 
+/* count_jobs' checks of the mode and the radii, for the calls that return
+ * before counting (no query points): no allocation, at most KD_MAX_EDGES
+ * distinct squared radii kept */
+static int check_radii_mode(const double *radii, int nradii, int mode)
+{
+    double seen[KD_MAX_EDGES];
+    int k, j, m = 0;
+    if (mode != KD_MODE_MIXED && mode != KD_MODE_FP64) {
+        kd_set_error(KD_EINVAL, "unknown count mode %d", mode);
+        return KD_EINVAL;
+    }
+    for (k = 0; k < nradii; k++)
+        if (radii[k] < 0) {
+            kd_set_error(KD_ERADIUS, "negative radius %g", radii[k]);
+            return KD_ERADIUS;
+        }
+    for (k = 0; k < nradii; k++) {
+        const double v = radii[k] * radii[k];
+        if (v != v) continue;
+        for (j = 0; j < m && seen[j] != v; j++)
+            ;
+        if (j < m) continue;
+        if (m == KD_MAX_EDGES) {
+            kd_set_error(KD_EINVAL, "at most %d distinct radii per call", KD_MAX_EDGES);
+            return KD_EINVAL;
+        }
+        seen[m++] = v;
+    }
+    return KD_OK;
+}
+
 /* query catalog from raw points; NaN rows are dropped (they count nothing in
  * the reference: every comparison with NaN is false, kdquery.c:33, :101-109) */
 static int query_catalog(const double *xyz, const int *fields, int n, int Fq, kd_catalog *qc,
@@ -374,6 +405,7 @@ int kd_count_points(kdtree_t tree, const double *xyz, const int *fields, int len
         return KD_EFIELD;
     }
     if (length == 0) {
+        if ((rc = check_radii_mode(radii, nradii, mode)) != KD_OK) return rc;
         if (nradii > 0)
             memset(out, 0, sizeof(long long) * (size_t)num_fields * (size_t)tree.num_fields *
                                (size_t)nradii);
@@ -384,6 +416,7 @@ int kd_count_points(kdtree_t tree, const double *xyz, const int *fields, int len
     rc = query_catalog(xyz, fields, length, num_fields, &qc, &empty);
     if (rc != KD_OK) return rc;
     if (empty) {
+        if ((rc = check_radii_mode(radii, nradii, mode)) != KD_OK) return rc;
         if (nradii > 0)
             memset(out, 0, sizeof(long long) * (size_t)num_fields * (size_t)tree.num_fields *
                                (size_t)nradii);
@@ -550,7 +583,9 @@ int kd_count_radii_static(kdtree_t tree, kdtree_t query, const double *radii, in
             if (uniq[j] == v) edge_of[k] = j;
     }
     if (ne == 0) {
-        memset(out, 0, sizeof(long long) * (size_t)nradii * query.num_fields * tree.num_fields);
+        if (nradii > 0)
+            memset(out, 0, sizeof(long long) * (size_t)nradii * (size_t)query.num_fields *
+                               (size_t)tree.num_fields);
         return KD_OK;
     }
     return kdg_count_static(&ht->cat, tree.num_fields, &hq->cat, query.num_fields, uniq, ne,

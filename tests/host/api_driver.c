@@ -11,7 +11,11 @@
  *             allocator that fails each allocation in turn (run under
  *             AddressSanitizer, which also reports leaks);
  *   coords  - the threaded RA/DEC conversion (coords_api.c), three callers
- *             at once, against a single-threaded evaluation.
+ *             at once, against a single-threaded evaluation;
+ *   fuzz    - 4,000 calls of the counting entry points with random counts,
+ *             radii, modes, field counts, NULL arrays and dead handles: each
+ *             succeeds exactly when the argument rules say it must, and then
+ *             with the brute-force counts (run under AddressSanitizer).
  * Prints PASS/FAIL lines; the exit status is the number of failures.
  */
 #include <math.h>
@@ -338,6 +342,145 @@ static void scenario_coords(void)
     printf("PASS coords\n");
 }
 
+/* ---- fuzz: random arguments, valid and not, through every counting entry
+ * point.  An independent statement of the argument rules predicts whether a
+ * call must succeed; it must then give the brute-force counts, and otherwise
+ * return a negative code.  Run under ASAN/UBSAN: no call may touch memory
+ * it should not. */
+
+/* distinct non-NaN squared radii among the first n, or -1 if one is negative */
+static int distinct_edges(const double *r, int n)
+{
+    double u[128];
+    int k, j, m = 0;
+    for (k = 0; k < n; k++) {
+        const double v = r[k] * r[k];
+        if (r[k] < 0) return -1;
+        if (v != v) continue;
+        for (j = 0; j < m && u[j] != v; j++)
+            ;
+        if (j == m) u[m++] = v;
+    }
+    return m;
+}
+
+/* the reference's counter holds every (qfield, tfield) of these catalogs */
+static int layout_ok(const cat_t *t, const cat_t *q)
+{
+    int i, mq = 0, mt = 0;
+    for (i = 0; i < q->n; i++) mq = q->f[i] > mq ? q->f[i] : mq;
+    for (i = 0; i < t->n; i++) mt = t->f[i] > mt ? t->f[i] : mt;
+    return (long long)mq * q->nf + mt < (long long)q->nf * t->nf;
+}
+
+static void scenario_fuzz(void)
+{
+    cat_t a = make_cat(60, 2), b = make_cat(90, 3), c = make_cat(40, 1);
+    cat_t *cats[3] = {&a, &b, &c};
+    kdtree_t tr[3], dead;
+    long long *out = (long long *)malloc(sizeof(long long) * 8192);
+    long long *want = (long long *)malloc(sizeof(long long) * 8192);
+    long long *cum = (long long *)malloc(sizeof(long long) * 8192);
+    double radii[80];
+    int it, i, k, succeeded = 0, refused = 0;
+    for (i = 0; i < 3; i++)
+        tr[i] = tree_construct(cats[i]->xyz, cats[i]->f, cats[i]->n, cats[i]->nf);
+    memset(&dead, 0, sizeof dead);
+    for (it = 0; it < 4000; it++) {
+        const int ti = (int)(urand() * 3), qi = (int)(urand() * 3), which = (int)(urand() * 5);
+        const cat_t *T = cats[ti], *Q = cats[qi];
+        const int nr = (int)(urand() * 75) - 5; /* -5 .. 69 */
+        const int mode = urand() < 0.9 ? (int)(urand() * 2) : (int)(urand() * 7) - 3;
+        const int null_r = urand() < 0.05, null_o = urand() < 0.05, bad_tree = urand() < 0.03;
+        const double *R = null_r ? NULL : radii;
+        long long *O = null_o ? NULL : out;
+        const kdtree_t tt = bad_tree ? dead : tr[ti];
+        const int Fq = Q->nf, Ft = T->nf;
+        int rc, ne, expect_ok;
+        for (k = 0; k < 80; k++) {
+            const double u = urand();
+            radii[k] = u < 0.05 ? NAN : u < 0.08 ? INFINITY : u < 0.095 ? -0.1 : urand() * 0.5;
+        }
+        ne = nr > 0 && !null_r ? distinct_edges(radii, nr) : 0;
+        /* rules shared by every entry point */
+        expect_ok = !bad_tree && nr >= 0 && (nr == 0 || (!null_r && !null_o)) &&
+                    (mode == 0 || mode == 1) && ne >= 0 && ne <= 64;
+        memset(out, 0x5a, sizeof(long long) * 8192);
+        switch (which) {
+        case 0: /* kd_count_radii */
+            expect_ok = expect_ok && layout_ok(T, Q);
+            rc = kd_count_radii(tt, tr[qi], R, nr, mode, O, NULL);
+            if (rc == 0 && expect_ok) {
+                brute(T, Q, radii, nr, want);
+                CHECK(same(out, want, (size_t)nr * Fq * Ft), "fuzz %d radii counts", it);
+            }
+            break;
+        case 1: { /* kd_count_points with a possibly bad length or field count */
+            const double u = urand();
+            const int len = u < 0.05 ? -3 : u < 0.12 ? 0 : Q->n;
+            const int fq = urand() < 0.05 ? (int)(urand() * 3) - 2 : Fq;
+            expect_ok = expect_ok && len >= 0 && fq >= 1 && (len == 0 || layout_ok(T, Q));
+            rc = kd_count_points(tt, Q->xyz, Q->f, len, fq, R, nr, mode, O, NULL);
+            if (rc == 0 && expect_ok) {
+                if (len == 0) memset(want, 0, sizeof(long long) * (size_t)nr * Fq * Ft);
+                else brute(T, Q, radii, nr, want);
+                CHECK(same(out, want, (size_t)nr * Fq * Ft), "fuzz %d point counts", it);
+            }
+            break;
+        }
+        case 2: /* kd_count_bins: at least one edge, arrays required */
+            expect_ok = expect_ok && nr >= 1 && !null_r && !null_o && layout_ok(T, Q);
+            rc = kd_count_bins(tt, tr[qi], R, nr, mode, O, NULL);
+            if (rc == 0 && expect_ok) {
+                brute(T, Q, radii, nr, cum);
+                for (k = 0; k + 1 < nr; k++)
+                    for (i = 0; i < Fq * Ft; i++)
+                        want[k * Fq * Ft + i] = cum[(k + 1) * Fq * Ft + i] - cum[k * Fq * Ft + i];
+                CHECK(same(out, want, (size_t)(nr - 1) * Fq * Ft), "fuzz %d bins", it);
+            }
+            break;
+        case 3: { /* kd_count_batch: jobs (T, Q) and (Q, T); output always required */
+            const kdtree_t ts[2] = {tt, tr[qi]}, qs[2] = {tr[qi], tr[ti]};
+            const int nj = urand() < 0.05 ? 0 : 2;
+            expect_ok = expect_ok && nj == 2 && !null_o && layout_ok(T, Q) && layout_ok(Q, T);
+            rc = kd_count_batch(ts, qs, nj, R, nr, mode, O, NULL);
+            if (rc == 0 && expect_ok) {
+                const size_t n0 = (size_t)nr * Fq * Ft;
+                brute(T, Q, radii, nr, want);
+                brute(Q, T, radii, nr, want + n0);
+                CHECK(same(out, want, 2 * n0), "fuzz %d batch", it);
+            }
+            break;
+        }
+        default: /* kd_count_radii_static: at most 64 radii */
+            expect_ok = expect_ok && nr <= 64 && layout_ok(T, Q);
+            rc = kd_count_radii_static(tt, tr[qi], R, nr, mode, O);
+            if (rc == 0 && expect_ok) {
+                brute(T, Q, radii, nr, want);
+                CHECK(same(out, want, (size_t)nr * Fq * Ft), "fuzz %d static", it);
+            }
+            break;
+        }
+        CHECK(rc <= 0, "fuzz %d: positive return %d", it, rc);
+        CHECK((rc == 0) == (expect_ok != 0), "fuzz %d (entry %d, nr %d, mode %d, ne %d): rc %d", it,
+              which, nr, mode, ne, rc);
+        if (rc == 0) succeeded++;
+        else refused++;
+    }
+    CHECK(succeeded > 1000 && refused > 500, "fuzz mix: %d succeeded, %d refused", succeeded,
+          refused);
+    for (i = 0; i < 3; i++) {
+        destroy(tr[i]);
+        free(cats[i]->xyz);
+        free(cats[i]->f);
+    }
+    free(out);
+    free(want);
+    free(cum);
+    printf("%s fuzz (%d calls succeeded, %d refused)\n", failures ? "FAIL" : "PASS", succeeded,
+           refused);
+}
+
 int main(int argc, char **argv)
 {
     int i;
@@ -346,6 +489,7 @@ int main(int argc, char **argv)
         else if (!strcmp(argv[i], "threads")) scenario_threads();
         else if (!strcmp(argv[i], "faults")) scenario_faults();
         else if (!strcmp(argv[i], "coords")) scenario_coords();
+        else if (!strcmp(argv[i], "fuzz")) scenario_fuzz();
     }
     printf("%d failures\n", failures);
     return failures;

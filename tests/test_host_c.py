@@ -5,8 +5,9 @@ count over the stored points); tests/host/api_driver.c drives the real C
 ABI: counts against an independent brute force, eight threads building,
 counting and destroying trees at once and three callers of the threaded
 RA/DEC conversion under ThreadSanitizer, and argument
-errors, injected device-layer failures and every allocation failing in turn
-under AddressSanitizer + UndefinedBehaviorSanitizer (leaks included)."""
+errors, injected device-layer failures, every allocation failing in turn and
+4,000 calls with random (valid and invalid) arguments under AddressSanitizer +
+UndefinedBehaviorSanitizer (leaks included)."""
 import os
 import shutil
 import subprocess
@@ -57,7 +58,7 @@ def test_host_library_under_thread_sanitizer(tmp_path):
 
 def test_host_library_under_address_sanitizer(tmp_path):
     exe = _build(tmp_path, "address,undefined", "asan")
-    out = _run(exe, "count", "faults",
+    out = _run(exe, "count", "faults", "fuzz",
                env={"ASAN_OPTIONS": "detect_leaks=1:halt_on_error=1",
                     "UBSAN_OPTIONS": "halt_on_error=1:print_stacktrace=1"})
-    assert "PASS count" in out and "PASS faults" in out
+    assert "PASS count" in out and "PASS faults" in out and "PASS fuzz" in out
