@@ -134,6 +134,33 @@ def test_oracle_matches_live_reference_random():
         R.destroy(rt)
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("scale", [1e-300, 1e-150, 1e100, 1e154, 1e155, 1e200, 1e300, 1.7e308])
+def test_oracle_matches_live_reference_at_extreme_magnitudes(scale):
+    """Coordinates from 1e-300 to 1.7e308: the variance sums of the split
+    choice underflow or overflow to inf (kdbuild.c:308-351) and the squared
+    distances of the counts overflow; the oracle still builds the
+    reference's node array and counts what the reference counts."""
+    R = O.RefLib()
+    rs = np.random.RandomState(51)
+    p = (rs.rand(500, 3) - 0.5) * scale
+    p[::7] *= 0.5 ** rs.randint(0, 40, len(p[::7]))[:, None]
+    f = (rs.rand(len(p)) * 3).astype(np.int32)
+    rt = R.build(p, f, 3)
+    try:
+        ot = O.OracleTree(p, f, 3)
+        rn, on = R.nodes(rt), ot.nodes()
+        assert np.array_equal(rn["xyz"].view(np.int64), on["xyz"].view(np.int64))
+        for k in ("field", "weight", "has_l", "has_r", "dim"):
+            assert np.array_equal(rn[k], on[k]), k
+        q = np.concatenate([p[:100], (rs.rand(50, 3) - 0.5) * scale])
+        qf = (rs.rand(len(q)) * 3).astype(np.int32)
+        for r in (0.0, 0.01 * scale, 0.3 * scale, 2.0 * scale, np.inf):
+            assert np.array_equal(R.pair_count(rt, q, qf, 3, r), ot.pair_count(q, qf, 3, r)), r
+    finally:
+        R.destroy(rt)
+
+
 def test_heap_rule_holds_and_catches_a_planted_violation(golden):
     """The reference's verify_tree rule holds on oracle trees (golden sets
     and a 200k lattice with ties), and fails once a child is moved to the
