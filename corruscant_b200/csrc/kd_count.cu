@@ -54,6 +54,13 @@ constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
 constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
 constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
 constexpr int kRunPerLane = KD_RUN_MAX / 32;  // staged run points per lane
+// FP32 tiles only where every staged value and square stays far inside FP32
+// range: tree and query points within kFp32Span of the block centre (their
+// squares and products below 1e30 < FLT_MAX) and squared edges below 1e30.
+// Records beyond that (coordinates or radii of 1e15 and more) are counted
+// by the exact FP64 path, as infinite radii are.
+constexpr double kFp32Span = 1e15;
+constexpr double kFp32MaxR = 1e30;
 // A run's exact counts travel one per byte (recounts) and its FP32 band sums
 // stay small (at most 4 * KD_RUN_MAX terms in [0, 1]): both need short runs.
 static_assert(KD_RUN_MAX % 32 == 0 && KD_RUN_MAX <= 128, "runs of 32..128 points");
@@ -498,6 +505,7 @@ template <int MODE> struct WarpSmem {
     JobDesc job;  // the job of the block being counted
     float Aw[KD_MAX_EDGES];
     float nsl[KD_MAX_EDGES];
+    double cmax2;  // squared leaf-centre distance below which FP32 is safe
     int uq[kMaxDistinctQf];
     float4 stage[MODE == KD_MODE_MIXED ? 2 * KD_RUN_MAX : 1];  // (X,X,Y,Y), (Z,Z,N,N)
     double stage64[MODE == KD_MODE_FP64 ? 3 * KD_RUN_MAX : 1];
@@ -599,6 +607,12 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             const double hx = 0.5 * (bx[3] - bx[0]), hy = 0.5 * (bx[4] - bx[1]),
                          hz = 0.5 * (bx[5] - bx[2]);
             const double Rq = sqrt(hx * hx + hy * hy + hz * hz) * (1.0 + 1e-12);
+            if (lane == 0) {
+                // |t' - o| <= |c - o| + hT and |q' - o| <= Rq must stay
+                // within kFp32Span (NaN box: never)
+                const double lim = kFp32Span - J.hT - Rq;
+                ws->cmax2 = lim > 0 ? lim * lim : -1.0;
+            }
             for (int k = lane; k < ne; k += 32) {
                 if (isfinite(R[k])) {
                     const double inv4e = 0.25 / band_halfwidth(R[k], Rq, J.hT);
@@ -697,9 +711,12 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             const int rs = (int)rec.x, rl = rec.z & 0xFF, tf = (rec.z >> 8) & 0xFF;
             const int k0 = (rec.z >> 16) & 0xFF, K = rec.z >> 24;
             // commit the staged run
+            bool fp32_range = false;
             if (K != 0) {
                 if (MODE == KD_MODE_MIXED) {
-                    const float dx = (float)(ncx - ox), dy = (float)(ncy - oy), dz = (float)(ncz - oz);
+                    const double ex = ncx - ox, ey = ncy - oy, ez = ncz - oz;
+                    fp32_range = ex * ex + ey * ey + ez * ez < ws->cmax2;
+                    const float dx = (float)ex, dy = (float)ey, dz = (float)ez;
 #pragma unroll
                     for (int h = 0; h < kRunPerLane; h++) {
                         const int j = lane + 32 * h;
@@ -747,7 +764,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                 continue;
             }
             wtiles++;
-            const bool fp32 = MODE == KD_MODE_MIXED && isfinite(R[k0 + K - 1]);
+            const bool fp32 = MODE == KD_MODE_MIXED && fp32_range && R[k0 + K - 1] < kFp32MaxR;
             // packed cumulative count of the previous edge, per query pair
             unsigned prev[kQ / 2];
 #pragma unroll
