@@ -23,6 +23,7 @@ Outputs (all small):
                    fields; seeded inputs): counts, every estimator x error
                    type and the reference's printed results tables
 """
+import atexit
 import hashlib
 import os
 import shutil
@@ -167,6 +168,7 @@ def _ref_python(ref_root):
     if "clustering" in _REF_PY:
         return _REF_PY["clustering"]
     tmp = tempfile.mkdtemp(prefix="refpy_")
+    atexit.register(shutil.rmtree, tmp, True)
     shutil.copytree(os.path.join(ref_root, "corruscant"), os.path.join(tmp, "corruscant"))
     os.makedirs(os.path.join(tmp, "corruscant", "bin"), exist_ok=True)
     for lib in ("libkdtree.so", "libcoords.so"):

@@ -50,7 +50,7 @@ def test_reference_arm_line():
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")
-def test_reference_arm_under_torchrun_prints_once():
+def test_reference_arm_under_torchrun_prints_once(tmp_path):
     """Launched like the multi-GPU runs (torchrun, 2 ranks): rank 0 alone
     runs the CPU reference and prints one line; the other rank exits 0."""
     import socket
@@ -62,7 +62,8 @@ def test_reference_arm_under_torchrun_prints_once():
          "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl",
          "reference", "--gpus", "2", "--scale", "0.01", "--steps", "1", "--warmup", "0",
          "--cpu-queries", "200"],
-        capture_output=True, text=True, timeout=600, cwd=HERE)
+        capture_output=True, text=True, timeout=600, cwd=HERE,
+        env={**os.environ, "TMPDIR": str(tmp_path)})  # torchrun's scratch stays here
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1, out.stdout[-2000:]
