@@ -1,8 +1,12 @@
-"""Input validation behaves like the reference's own functions, run side by
-side (the reference's Python package imported from a temporary copy, as
-tests/golden/make_golden.py does; skipped where the reference or its build
-is absent): same result arrays and dtypes, same copy warnings, same
-exception types and messages, for well-formed and malformed inputs."""
+"""The reference's own Python functions run side by side with ours (its
+package imported from a temporary copy, as tests/golden/make_golden.py does;
+skipped where the reference or its build is absent).
+
+Input validation: same result arrays and dtypes, same copy warnings, same
+exception types and messages, for well-formed and malformed inputs.
+Results classes: random count arrays of several field and bin counts, auto
+and cross, give the same estimates, errors (bootstrap seeded), covariances
+and printed tables, bit for bit."""
 import importlib.util
 import os
 import warnings
@@ -76,3 +80,48 @@ def test_validate_fields_like_reference(ref, fname):
     pts = np.ascontiguousarray(rs.rand(12, 3))
     f = FIELDS[fname](12)
     assert _outcome(clustering.validate_fields, f, pts) == _outcome(ref.validate_fields, f, pts)
+
+
+def _tree_attrs(sizes):
+    import types
+    return types.SimpleNamespace(N_fields=len(sizes), field_sizes=np.asarray(sizes))
+
+
+@pytest.mark.parametrize("F,nb,cross", [(2, 1, False), (5, 4, False), (13, 9, False),
+                                        (3, 5, True), (8, 2, True)])
+def test_results_like_reference(ref, F, nb, cross):
+    """Random count arrays through our results classes and the reference's:
+    every estimator x error type, covariances and tables, bit for bit."""
+    g = np.random.RandomState(100 + F * 10 + nb)
+    n = 4 if cross else 3
+    arrays = [g.randint(0, 10 ** k, (nb, F, F)).astype(np.int64) for k in (4, 5, 6, 7)[:n]]
+    arrays[-1] += 1
+    sizes = [g.randint(1, 10 ** 4, F) for _ in range(4)]
+    trees = [_tree_attrs(s) for s in sizes]
+    radii = np.logspace(-2, -1, nb + 1)
+    objs = []
+    for mod in (clustering, ref):
+        if cross:
+            r = mod.crosscorr_results(*[a.copy() for a in arrays], *trees, mod.est_landy_szalay,
+                                      radii)
+        else:
+            r = mod.autocorr_results(*[a.copy() for a in arrays], trees[0], trees[1],
+                                     mod.est_landy_szalay, radii)
+        r.radii_nominal, r.radii_units = radii, "Data units"
+        objs.append((mod, r))
+    for est in ("est_standard", "est_hamilton", "est_landy_szalay"):
+        outs = []
+        for mod, r in objs:
+            r.estimator = getattr(mod, est)
+            o = [_outcome(r.estimate)]
+            for err in (None, "poisson", "ftf", "jackknife", "bootstrap"):
+                np.random.seed(5)
+                o.append(_outcome(r.error, err))
+                r.error_type = err
+                np.random.seed(5)
+                o.append(_outcome(str, r))
+            for kind in ("jackknife", "ftf"):
+                for norm in (False, True):
+                    o.append(_outcome(r.covariance, kind, norm))
+            outs.append(o)
+        assert outs[0] == outs[1], est
