@@ -30,13 +30,18 @@ shapes; no dataset is involved):
 A step is every count of the workload for all edges: one kd_count_batch call
 on prebuilt trees, inputs resident in HBM.  value = pairs tested per second,
 all ranks, with the mixed FP32 + FP64-recheck counter; the plain FP64 counter
-is timed on the same steps.  e2e = the same pairs per second through the C ABI
-from host buffers: tree_construct of every catalog (H2D of the points, node
-arrays back to the host; for the angular workload the RA/DEC conversion too),
-the batched count, results read back, every step.  Also reported: the FP64
-form against a measured DGEMM peak, the all-pairs-equivalent rate (sum of
-Nq * Nt over the counts, per step time) and an FP32-pipe model of the binning
-(FMA lane-ops per pair from the measured active edges per pair).
+is timed on the same steps.  e2e = a full result end to end through the C ABI
+from pinned host buffers: tree_construct of every catalog (H2D of the points,
+node arrays back to the host; for the angular workload the RA/DEC conversion
+too), the batched count, results read back, every step; its value is in
+all-pairs-equivalent pairs per second (sum of Nq * Nt over the counts per
+second of a full result), the unit the reference arm's e2e uses too, so that
+their ratio is the ratio of times per full result.  Also reported: the FP64
+form against its CUDA-core peak, the time per full result and an FP32-pipe
+model of the binning (FMA lane-ops per pair from the measured active edges
+per pair).  The default run then measures the angular, mocks and lattice
+workloads at full size (a few steps each, both precisions, e2e, reference
+sample) under "other_workloads".
 
 --gpus N (torchrun): every rank builds the trees and counts its 1/N share of
 the batch's query blocks (kd_count_batch_shard); the per-rank counts are
@@ -65,6 +70,9 @@ sys.path.insert(0, HERE)
 
 METRIC = "pairs tested/s, exact counts: FP32+FP64-recheck vs plain FP64 on B200; CPU ref"
 UNIT = "pairs/s"
+# end-to-end rates of both arms: exhaustive-equivalent pairs (sum of Nq * Nt
+# over the counts) per second of a full result, comparable across algorithms
+E2E_UNIT = "all-pairs-equivalent pairs/s"
 FLOP_PER_PAIR = 8  # 3 subtractions, 1 multiply, 2 fused multiply-adds per distance
 
 # ---------------------------------------------------------------- workloads
@@ -422,11 +430,19 @@ def _pinned_copies(w):
     return host, keep
 
 
-def run_mine(args):
-    from corruscant_b200 import _native as N
-    D = Dist()
-    N.set_device(D.local)
-    w = WORKLOADS[args.workload](args.scale)
+def _all_pairs(w):
+    """Sum over the workload's counts of Nq * Nt (raw catalog sizes): the
+    pairs an exhaustive count would test, a unit that does not depend on the
+    algorithm (the reference and this engine test different pair sets)."""
+    sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
+    return float(sum(sizes[q] * sizes[t] for _, t, q in w.jobs))
+
+
+def _measure(N, D, w, steps, warmup):
+    """Time one workload: `steps` device-timed steps per precision after
+    `warmup` untimed ones (inputs resident in HBM), then `steps` end-to-end
+    steps from pinned host buffers.  Returns the raw figures, reduced over
+    ranks (device times: max; pairs: sum)."""
     radii = w.radii
     t0 = time.perf_counter()
     trees = _build_all(N, w)
@@ -448,7 +464,6 @@ def run_mine(args):
         acc = dict(dev_ms=0.0, pairs=0, launches=0, tile_launches=0, tiles_ms=0.0, rechecked=0,
                    edge_pairs=0)
         res = None
-        t0 = time.perf_counter()
         for _ in range(k):
             res, s = step(mode)
             acc["dev_ms"] += s["ms_total"]
@@ -458,24 +473,23 @@ def run_mine(args):
             acc["tiles_ms"] += s["ms_tiles"]
             acc["rechecked"] += s["pairs_rechecked"]
             acc["edge_pairs"] += s["edge_pairs"]
-        acc["wall"] = time.perf_counter() - t0
         acc["res"] = res
         D.barrier()
         return acc
 
-    peak = gemm_peak_tflops(D.local, "float32") if D.rank == 0 else None
-    peak64 = gemm_peak_tflops(D.local, "float64") if D.rank == 0 else None
     with ClockSampler(D.local) as clk:
-        mixed = timed(N.KD_MODE_MIXED, args.steps, args.warmup)
+        mixed = timed(N.KD_MODE_MIXED, steps, warmup)
     clocks = clk.summary()
-    fp64 = timed(N.KD_MODE_FP64, args.steps, max(1, args.warmup // 2))
+    fp64 = timed(N.KD_MODE_FP64, steps, max(1, warmup // 2))
 
     # exactness across ranks and modes: summed shard counts must agree
     tot_m = {k: D.reduce(v, "SUM") for k, v in mixed["res"].items()}
     tot_f = {k: D.reduce(v, "SUM") for k, v in fp64["res"].items()}
     exact = all(np.array_equal(tot_m[k], tot_f[k]) for k in tot_m)
 
-    # e2e through the C ABI from pinned host buffers, every step
+    # e2e through the C ABI from pinned host buffers, every step: tree
+    # builds (H2D of the points, node arrays back to the host, the RA/DEC
+    # conversion for sky catalogs), the batched count, results on the host
     for t in trees.values():
         N.destroy(t)
     host, _keep = _pinned_copies(w)
@@ -484,98 +498,177 @@ def run_mine(args):
     for name, (pts, f, _) in w.catalogs.items():
         h2d += (2 * 8 * len(pts) if name in w.radec else pts.nbytes) + (f.nbytes if f is not None else 0)
     d2h = 0
-    for it in range(1 + args.steps):
+    for it in range(1 + steps):
         D.barrier()
         t0 = time.perf_counter()
         tt = _build_all(N, w, convert=True, host=host)
         _, s = N.count_batch([(tt[t], tt[q]) for _, t, q in w.jobs], radii, with_stats=True,
                              shard=D.rank, nshards=D.world)
-        p = s["pairs_tested"]
         dt = time.perf_counter() - t0
         d2h = 40 * sum(t.memsize for t in tt.values()) + 8 * len(radii) * sum(
             tt[t].num_fields * tt[q].num_fields for _, t, q in w.jobs)
         for t in tt.values():
             N.destroy(t)
         if it > 0:  # the first iteration warms the allocator
-            e2e_pairs += p
+            e2e_pairs += s["pairs_tested"]
             e2e_wall += dt
+    del _keep
+    return dict(
+        build_s=build_s, clocks=clocks, exact=bool(exact), mixed=mixed, fp64=fp64,
+        dev_s=float(D.reduce([mixed["dev_ms"] * 1e-3], "MAX")[0]),
+        pairs=int(D.reduce([mixed["pairs"]], "SUM")[0]),
+        fdev_s=float(D.reduce([fp64["dev_ms"] * 1e-3], "MAX")[0]),
+        fpairs=int(D.reduce([fp64["pairs"]], "SUM")[0]),
+        e_wall=float(D.reduce([e2e_wall], "MAX")[0]),
+        e_pairs=int(D.reduce([e2e_pairs], "SUM")[0]),
+        rechecked=int(D.reduce([mixed["rechecked"]], "SUM")[0]),
+        h2d=int(h2d), d2h=int(d2h), pinned=host is not None)
 
-    dev_s = float(D.reduce([mixed["dev_ms"] * 1e-3], "MAX")[0])
-    pairs = int(D.reduce([mixed["pairs"]], "SUM")[0])
-    fdev_s = float(D.reduce([fp64["dev_ms"] * 1e-3], "MAX")[0])
-    fpairs = int(D.reduce([fp64["pairs"]], "SUM")[0])
-    e_wall = float(D.reduce([e2e_wall], "MAX")[0])
-    e_pairs = int(D.reduce([e2e_pairs], "SUM")[0])
-    rechecked = int(D.reduce([mixed["rechecked"]], "SUM")[0])
 
+def _fp64_lane_peak(device, mhz):
+    """FP64 CUDA-core peak at the sampled clock: SMs x 64 FP64 lanes x 2
+    FLOP (FMA) per clock.  The FP64 tiles run on that pipe, not on the FP64
+    tensor cores a DGEMM uses."""
+    nsm = sm_count(device)
+    return nsm * 64 * 2 * mhz * 1e6 / 1e12 if (nsm and mhz) else None
+
+
+def _summary(w, m, steps, peak, peak64, D):
+    """The figures of one measured workload (rank 0)."""
+    value = m["pairs"] / m["dev_s"]
+    all_pairs = _all_pairs(w)
+    s_full = m["dev_s"] / steps
+    e_s = m["e_wall"] / steps
+    mixed, fp64 = m["mixed"], m["fp64"]
+    # the dominant kernel: k_tiles, one launch per step (the whole batch)
+    launch_pairs = mixed["pairs"] / max(1, mixed["tile_launches"])
+    launch_ms = mixed["tiles_ms"] / max(1, mixed["tile_launches"])
+    achieved = launch_pairs * FLOP_PER_PAIR / (launch_ms * 1e-3) / 1e12
+    mhz = m["clocks"].get("sm_mhz")
+    nsm = sm_count(D.local)
+    lane32 = nsm * 128 * 2 * mhz * 1e6 / 1e12 if (nsm and mhz) else None
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if peak else None,
+                "traffic": TILE_TRAFFIC_PER_PAIR * launch_pairs if TILE_TRAFFIC_PER_PAIR else None,
+                "kernel": "k_tiles<mixed> (one launch: the step's whole batch)",
+                "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off",
+                "lane_peak": lane32,
+                "frac_of_lane_peak": (achieved / lane32) if lane32 else None,
+                "lane_peak_basis": "SMs x 128 FP32 lanes x 2 FLOP x median SM clock",
+                "flop_per_pair": FLOP_PER_PAIR}
+    if TILE_TRAFFIC_PER_PAIR:
+        roofline["traffic_source"] = TILE_TRAFFIC_SOURCE
+    # FP32-pipe model of the binning itself: per pair 3 FMA lane-ops for
+    # the distance and 3 per active edge (ramp, count, band check)
+    kbar = mixed["edge_pairs"] / max(1, mixed["pairs"])
+    ops = 3.0 + 3.0 * kbar
+    pipe_bound = 128.0 * nsm * mhz * 1e6 / ops if (nsm and mhz) else None
+    tile_rate = launch_pairs / (launch_ms * 1e-3)
+    pipe_model = {"active_edges_per_pair": kbar, "fma_lane_ops_per_pair": ops,
+                  "bound_pairs_per_s": pipe_bound,
+                  "frac": tile_rate / pipe_bound if pipe_bound else None,
+                  "basis": "128 FP32 lanes/SM/clock x SMs x median SM clock"}
+    f_launch_pairs = fp64["pairs"] / max(1, fp64["tile_launches"])
+    f_launch_ms = fp64["tiles_ms"] / max(1, fp64["tile_launches"])
+    f_achieved = f_launch_pairs * FLOP_PER_PAIR / (f_launch_ms * 1e-3) / 1e12
+    lane64 = _fp64_lane_peak(D.local, mhz)
+    fp64_roofline = {"bound": "fp64", "achieved": f_achieved, "peak": lane64,
+                     "unit": "TFLOP/s", "frac": (f_achieved / lane64) if lane64 else None,
+                     "kernel": "k_tiles<fp64>",
+                     "peak_source": "SMs x 64 FP64 lanes x 2 FLOP x median SM clock "
+                                    "(the FP64 CUDA-core pipe the kernel runs on)",
+                     "dgemm_measured": peak64}
+    return {
+        "value": value, "ms_per_step": s_full * 1e3, "s_per_full_result": s_full,
+        "fp64_form": {"value": m["fpairs"] / m["fdev_s"],
+                      "ms_per_step": m["fdev_s"] / steps * 1e3,
+                      "s_per_full_result": m["fdev_s"] / steps, "dtype": "f64",
+                      "roofline": fp64_roofline},
+        "all_pairs_equivalent_per_s": all_pairs / s_full,
+        "fp32_pipe_model": pipe_model,
+        "mixed_over_fp64": value / (m["fpairs"] / m["fdev_s"]),
+        "counts_exact_mixed_vs_fp64": m["exact"],
+        "recheck_rate": m["rechecked"] / max(1, m["pairs"]),
+        "pairs_rechecked_per_step": m["rechecked"] / steps,
+        "build_s": m["build_s"],
+        "roofline": roofline,
+        "e2e": {"value": all_pairs / e_s, "unit": E2E_UNIT,
+                "h2d_bytes_per_step": m["h2d"], "d2h_bytes_per_step": m["d2h"],
+                "s_per_step": e_s, "s_per_full_result": e_s,
+                "pairs_tested_per_s": m["e_pairs"] / m["e_wall"],
+                "host_buffers": "pinned" if m["pinned"] else "pageable"},
+        "clocks": m["clocks"],
+        "gpu_launches": int(mixed["launches"]),
+    }
+
+
+def _config(w, D):
+    sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
+    cfg = {"workload": w.description, "counts": len(w.jobs), "edges": len(w.radii),
+           "parallelism": f"query blocks sharded over {D.world} GPU(s)",
+           "l2": "inputs larger than L2 (tree points stream from HBM each step)"}
+    if len(sizes) <= 4:
+        cfg["catalogs"] = sizes
+    else:
+        cfg["catalog_points_total"] = int(sum(sizes.values()))
+        cfg["catalogs"] = len(sizes)
+    return cfg
+
+
+# the other BASELINE workloads measured by the default run after the headline
+OTHER_WORKLOADS = ("angular", "mocks", "lattice")
+OTHER_STEPS = 3
+
+
+def run_mine(args):
+    from corruscant_b200 import _native as N
+    D = Dist()
+    N.set_device(D.local)
+    w = WORKLOADS[args.workload](args.scale)
+    peak = gemm_peak_tflops(D.local, "float32") if D.rank == 0 else None
+    peak64 = gemm_peak_tflops(D.local, "float64") if D.rank == 0 else None
+    m = _measure(N, D, w, args.steps, args.warmup)
     if D.rank == 0:
-        value = pairs / dev_s
-        # the dominant kernel: k_tiles, one launch per step (the whole batch)
-        launch_pairs = mixed["pairs"] / max(1, mixed["tile_launches"])
-        launch_ms = mixed["tiles_ms"] / max(1, mixed["tile_launches"])
-        achieved = launch_pairs * FLOP_PER_PAIR / (launch_ms * 1e-3) / 1e12
-        roofline = {"bound": "fp32", "achieved": achieved,
-                    "peak": peak, "unit": "TFLOP/s",
-                    "frac": (achieved / peak) if peak else None,
-                    "traffic": TILE_TRAFFIC_PER_PAIR * launch_pairs
-                    if TILE_TRAFFIC_PER_PAIR else None,
-                    "kernel": "k_tiles<mixed> (one launch: the step's whole batch)",
-                    "peak_source": "measured in this run: cuBLAS SGEMM 8192^3, TF32 off",
-                    "flop_per_pair": FLOP_PER_PAIR}
-        if TILE_TRAFFIC_PER_PAIR:
-            roofline["traffic_source"] = TILE_TRAFFIC_SOURCE
-        # FP32-pipe model of the binning itself: per pair 3 FMA lane-ops for
-        # the distance and 3 per active edge (ramp, count, band check)
-        kbar = mixed["edge_pairs"] / max(1, mixed["pairs"])
-        nsm, mhz = sm_count(D.local), clocks.get("sm_mhz")
-        ops = 3.0 + 3.0 * kbar
-        pipe_bound = 128.0 * nsm * mhz * 1e6 / ops if (nsm and mhz) else None
-        tile_rate = launch_pairs / (launch_ms * 1e-3)
-        pipe_model = {"active_edges_per_pair": kbar, "fma_lane_ops_per_pair": ops,
-                      "bound_pairs_per_s": pipe_bound,
-                      "frac": tile_rate / pipe_bound if pipe_bound else None,
-                      "basis": "128 FP32 lanes/SM/clock x SMs x median SM clock"}
-        f_launch_pairs = fp64["pairs"] / max(1, fp64["tile_launches"])
-        f_launch_ms = fp64["tiles_ms"] / max(1, fp64["tile_launches"])
-        f_achieved = f_launch_pairs * FLOP_PER_PAIR / (f_launch_ms * 1e-3) / 1e12
-        fp64_roofline = {"bound": "fp64", "achieved": f_achieved, "peak": peak64,
-                         "unit": "TFLOP/s", "frac": (f_achieved / peak64) if peak64 else None,
-                         "kernel": "k_tiles<fp64>",
-                         "peak_source": "measured in this run: cuBLAS DGEMM 8192^3"}
-        sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
-        all_pairs = float(sum(sizes[q] * sizes[t] for _, t, q in w.jobs))
-        cfg = {"workload": w.description, "counts": len(w.jobs), "edges": len(radii),
-               "parallelism": f"query blocks sharded over {D.world} GPU(s)",
-               "l2": "inputs larger than L2 (tree points stream from HBM each step)"}
-        if len(sizes) <= 4:
-            cfg["catalogs"] = sizes
-        else:
-            cfg["catalog_points_total"] = int(sum(sizes.values()))
-            cfg["catalogs"] = len(sizes)
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": D.world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_s / args.steps * 1e3, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
-            "data": w.data, "config": cfg,
-            "fp64_form": {"value": fpairs / fdev_s, "ms_per_step": fdev_s / args.steps * 1e3,
-                          "dtype": "f64", "roofline": fp64_roofline},
-            "all_pairs_equivalent_per_s": all_pairs / (dev_s / args.steps),
-            "fp32_pipe_model": pipe_model,
-            "mixed_over_fp64": (pairs / dev_s) / (fpairs / fdev_s),
-            "counts_exact_mixed_vs_fp64": bool(exact),
-            "recheck_rate": rechecked / max(1, pairs),
-            "pairs_rechecked_per_step": rechecked / args.steps,
-            "build_s": build_s,
-            "roofline": roofline,
-            "e2e": {"value": e_pairs / e_wall, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "s_per_step": e_wall / args.steps,
-                    "host_buffers": "pinned" if host is not None else "pageable"},
-            "clocks": clocks,
-            "gpu_launches": int(mixed["launches"]),
-        }
+        line = {"metric": METRIC, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
+                "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32+f64", "data": w.data,
+                "config": _config(w, D)}
+        line.update(_summary(w, m, args.steps, peak, peak64, D))
+        line = {k: line[k] for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup",
+                                     "ms_per_step")} | line
         if D.world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(w, n_queries=args.cpu_queries, gpu=N)
+            cb = cpu_baseline(w, n_queries=args.cpu_queries, gpu=N)
+            line["cpu_baseline"] = cb
+            if cb.get("full_result_s_extrapolated"):
+                line["speedup_per_full_result"] = {
+                    "device": cb["full_result_s_extrapolated"] / line["s_per_full_result"],
+                    "e2e": cb["full_result_s_extrapolated"] / line["e2e"]["s_per_full_result"]}
+    # the other workloads at full size (one GPU, default workload only): a
+    # few steps each, both precisions, e2e and the reference sample
+    others = {}
+    if D.world == 1 and args.workload == "clustered3d" and args.scale == 1.0 and not args.headline_only:
+        del m
+        for name in OTHER_WORKLOADS:
+            wo = WORKLOADS[name](1.0)
+            mo = _measure(N, D, wo, OTHER_STEPS, 3)
+            o = _summary(wo, mo, OTHER_STEPS, peak, peak64, D)
+            o = {"config": _config(wo, D), "steps": OTHER_STEPS, "warmup": 3} | {
+                k: o[k] for k in ("value", "ms_per_step", "s_per_full_result", "fp64_form",
+                                  "mixed_over_fp64", "counts_exact_mixed_vs_fp64", "recheck_rate",
+                                  "all_pairs_equivalent_per_s", "roofline", "fp32_pipe_model",
+                                  "e2e", "clocks", "build_s")}
+            if not args.no_cpu_baseline:
+                cb = cpu_baseline(wo, n_queries=args.cpu_queries, gpu=N)
+                o["cpu_baseline"] = cb
+                if cb.get("full_result_s_extrapolated"):
+                    o["speedup_per_full_result"] = {
+                        "device": cb["full_result_s_extrapolated"] / o["s_per_full_result"],
+                        "e2e": cb["full_result_s_extrapolated"] / o["e2e"]["s_per_full_result"]}
+            others[name] = o
+            del wo, mo
+    if D.rank == 0:
+        if others:
+            line["other_workloads"] = others
         print(json.dumps(line), flush=True)
     D.close()
 
@@ -664,7 +757,9 @@ def cpu_baseline(w, n_queries=None, steps=1, warmup=0, gpu=None):
            "cores": max(1, min(cores, nq_max // 20)), "kind": "reference",
            "sample": (f"{'/'.join(map(str, nsamp))} seeded query points for each of the "
                       f"{len(samples)} counts against the full trees, {len(w.radii)} "
-                      f"pair_count calls per count"),
+                      f"pair_count calls per count; the sample is sized for 10-30 s of "
+                      f"CPU work (a 1% query subset would take minutes per count), and "
+                      f"the time per full result is extrapolated linearly in the queries"),
            "s_per_sample": t_all, "pairs_tested_per_sample": int(visits),
            "full_result_s_extrapolated": full_s,
            "note": "pairs tested on the CPU = reference traversal node visits"}
@@ -692,15 +787,21 @@ def run_reference(args):
         cfg["catalogs"] = sizes
     else:
         cfg["catalogs"] = len(sizes)
+    full_s = cb["full_result_s_extrapolated"]
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": cb["s_per_sample"] * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "f64", "data": w.data, "config": cfg,
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "full_result_s_extrapolated": cb["full_result_s_extrapolated"],
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
+            "s_per_full_result": full_s,
+            "full_result_s_extrapolated": full_s,
+            "all_pairs_equivalent_per_s": _all_pairs(w) / full_s,
+            # end to end: a full result's exhaustive-equivalent pairs per
+            # second of (extrapolated) CPU time, the unit of the GPU arm's e2e
+            "e2e": {"value": _all_pairs(w) / full_s, "unit": E2E_UNIT,
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                    "s_per_full_result": full_s}}
     print(json.dumps(line), flush=True)
 
 
@@ -715,6 +816,8 @@ def main():
     ap.add_argument("--cpu-queries", type=int, default=None,
                     help="query points per count in the CPU sample (default per workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="skip the other workloads after the default one")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "mine":
         ap.error("at least 3 warm-up steps")

@@ -187,18 +187,41 @@ static int cmp_double(const void *a, const void *b)
     return x < y ? -1 : (x > y ? 1 : 0);
 }
 
+/* add a pass's statistics to the call's totals */
+static void add_stats(kd_count_stats *to, const kd_count_stats *s)
+{
+    to->pairs_tested += s->pairs_tested;
+    to->pairs_rechecked += s->pairs_rechecked;
+    to->pairs_accepted += s->pairs_accepted;
+    to->pairs_wide += s->pairs_wide;
+    to->edge_pairs += s->edge_pairs;
+    to->warp_tiles += s->warp_tiles;
+    to->entries += s->entries;
+    to->ms_traverse += s->ms_traverse;
+    to->ms_tiles += s->ms_tiles;
+    to->ms_total += s->ms_total;
+    to->tile_launches += s->tile_launches;
+    to->launches += s->launches;
+}
+
 /*
- * Count njobs (tree catalog, query catalog) pairs for all radii in one device
- * batch and write, job after job, the reference's cumulative per-radius
- * matrices out[k][qf*Fq + tf] (kdquery.c:34: rows strided by the QUERY field
- * count Fq), nradii * Fq[j] * Ft[j] values per job.
+ * Count njobs (tree catalog, query catalog) pairs for all radii and write,
+ * job after job, the reference's cumulative per-radius matrices
+ * out[k][qf*Fq + tf] (kdquery.c:34: rows strided by the QUERY field count
+ * Fq), nradii * Fq[j] * Ft[j] values per job.
+ *
+ * The distinct squared radii are counted in passes of at most KD_MAX_EDGES
+ * (ascending), each one device batch over all jobs.  A pair's count at a
+ * radius depends on that radius alone, so the passes are independent and any
+ * number of radii gives the reference's counts (its drivers call pair_count
+ * once per radius, clustering.py:218-230, whatever their number).
  */
 static int count_jobs(const kd_catalog *const *tcs, const int *Fts, const kd_catalog *const *qcs,
                       const int *Fqs, int njobs, const double *radii, int nradii, int mode,
                       int shard, int nshards, long long *out, kd_count_stats *stats)
 {
     double *rsq = NULL, *uniq = NULL;
-    long long **hists = NULL;
+    long long **hists = NULL, **cums = NULL;
     int j, k, ne = 0, rc = KD_OK;
     size_t total = 0;
 
@@ -234,7 +257,8 @@ static int count_jobs(const kd_catalog *const *tcs, const int *Fts, const kd_cat
     rsq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
     uniq = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
     hists = (long long **)calloc((size_t)njobs, sizeof(long long *));
-    if (!rsq || !uniq || !hists) {
+    cums = (long long **)calloc((size_t)njobs, sizeof(long long *));
+    if (!rsq || !uniq || !hists || !cums) {
         kd_set_error(KD_ENOMEM, "out of host memory");
         rc = KD_ENOMEM;
         goto done;
@@ -250,32 +274,53 @@ static int count_jobs(const kd_catalog *const *tcs, const int *Fts, const kd_cat
             if (w == 0 || uniq[k] != uniq[w - 1]) uniq[w++] = uniq[k];
         ne = w;
     }
-    if (ne > KD_MAX_EDGES) {
-        kd_set_error(KD_EINVAL, "at most %d distinct radii per call", KD_MAX_EDGES);
-        rc = KD_EINVAL;
-        goto done;
-    }
     if (ne == 0) goto done;
     for (j = 0; j < njobs; j++) {
         const size_t hrow = ((size_t)qcs[j]->max_qf + 1) * ((size_t)tcs[j]->max_tf + 1);
-        hists[j] = (long long *)calloc((size_t)(ne + 1) * hrow, sizeof(long long));
-        if (!hists[j]) {
+        const int npass = ne < KD_MAX_EDGES ? ne : KD_MAX_EDGES;
+        hists[j] = (long long *)calloc((size_t)(npass + 1) * hrow, sizeof(long long));
+        cums[j] = (long long *)calloc((size_t)ne * hrow, sizeof(long long));
+        if (!hists[j] || !cums[j]) {
             kd_set_error(KD_ENOMEM, "out of host memory");
             rc = KD_ENOMEM;
             goto done;
         }
     }
-    rc = kdg_count_batch(tcs, qcs, njobs, uniq, ne, mode, shard, nshards, hists, stats);
-    if (rc != KD_OK) goto done;
+    {
+        int e0;
+        for (e0 = 0; e0 < ne; e0 += KD_MAX_EDGES) {
+            const int n = ne - e0 < KD_MAX_EDGES ? ne - e0 : KD_MAX_EDGES;
+            kd_count_stats ps;
+            memset(&ps, 0, sizeof ps);
+            if (e0 > 0)
+                for (j = 0; j < njobs; j++)
+                    memset(hists[j], 0, sizeof(long long) * (size_t)(n + 1) *
+                                            ((size_t)qcs[j]->max_qf + 1) *
+                                            ((size_t)tcs[j]->max_tf + 1));
+            rc = kdg_count_batch(tcs, qcs, njobs, uniq + e0, n, mode, shard, nshards, hists,
+                                 stats ? &ps : NULL);
+            if (rc != KD_OK) goto done;
+            if (stats) add_stats(stats, &ps);
+            /* hist[e] holds the pairs with uniq[e0+e-1] <= d2 < uniq[e0+e]
+             * (e = 0: every pair below uniq[e0]); cumulative sums give the
+             * pairs with d2 < uniq[e0+e] */
+            for (j = 0; j < njobs; j++) {
+                const size_t hrow = ((size_t)qcs[j]->max_qf + 1) * ((size_t)tcs[j]->max_tf + 1);
+                const long long *h = hists[j];
+                long long *c = cums[j] + (size_t)e0 * hrow;
+                size_t i;
+                int e;
+                for (i = 0; i < hrow; i++) c[i] = h[i];
+                for (e = 1; e < n; e++)
+                    for (i = 0; i < hrow; i++)
+                        c[(size_t)e * hrow + i] = c[(size_t)(e - 1) * hrow + i] + h[(size_t)e * hrow + i];
+            }
+        }
+    }
     for (j = 0; j < njobs; j++) {
         const size_t Fqe = (size_t)qcs[j]->max_qf + 1, Fte = (size_t)tcs[j]->max_tf + 1;
         const size_t hrow = Fqe * Fte, nrow = (size_t)Fqs[j] * (size_t)Fts[j];
-        long long *hist = hists[j];
-        /* cumulative over sorted edges: pairs with d2 < uniq[e] */
-        for (k = 1; k < ne; k++) {
-            size_t i;
-            for (i = 0; i < hrow; i++) hist[(size_t)k * hrow + i] += hist[(size_t)(k - 1) * hrow + i];
-        }
+        const long long *cum = cums[j];
         for (k = 0; k < nradii; k++) {
             int lo = 0, hi = ne;
             size_t qf, tf;
@@ -288,14 +333,17 @@ static int count_jobs(const kd_catalog *const *tcs, const int *Fts, const kd_cat
             }
             for (qf = 0; qf < Fqe; qf++)
                 for (tf = 0; tf < Fte; tf++)
-                    o[qf * (size_t)Fqs[j] + tf] += hist[(size_t)lo * hrow + qf * Fte + tf];
+                    o[qf * (size_t)Fqs[j] + tf] += cum[(size_t)lo * hrow + qf * Fte + tf];
         }
         out += nrow * (size_t)nradii;
     }
 done:
     if (hists)
         for (j = 0; j < njobs; j++) free(hists[j]);
+    if (cums)
+        for (j = 0; j < njobs; j++) free(cums[j]);
     free(hists);
+    free(cums);
     free(rsq);
     free(uniq);
     return rc;
@@ -309,12 +357,10 @@ static int count_catalogs(const kd_catalog *tc, int Ft, const kd_catalog *qc, in
 }
 
 /* count_jobs' checks of the mode and the radii, for the calls that return
- * before counting (no query points): no allocation, at most KD_MAX_EDGES
- * distinct squared radii kept */
+ * before counting (no query points) */
 static int check_radii_mode(const double *radii, int nradii, int mode)
 {
-    double seen[KD_MAX_EDGES];
-    int k, j, m = 0;
+    int k;
     if (mode != KD_MODE_MIXED && mode != KD_MODE_FP64) {
         kd_set_error(KD_EINVAL, "unknown count mode %d", mode);
         return KD_EINVAL;
@@ -324,18 +370,6 @@ static int check_radii_mode(const double *radii, int nradii, int mode)
             kd_set_error(KD_ERADIUS, "negative radius %g", radii[k]);
             return KD_ERADIUS;
         }
-    for (k = 0; k < nradii; k++) {
-        const double v = radii[k] * radii[k];
-        if (v != v) continue;
-        for (j = 0; j < m && seen[j] != v; j++)
-            ;
-        if (j < m) continue;
-        if (m == KD_MAX_EDGES) {
-            kd_set_error(KD_EINVAL, "at most %d distinct radii per call", KD_MAX_EDGES);
-            return KD_EINVAL;
-        }
-        seen[m++] = v;
-    }
     return KD_OK;
 }
 

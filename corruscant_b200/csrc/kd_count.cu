@@ -1222,7 +1222,9 @@ void *g_static_ptr[kMaxDevices];  // device address of g_static_scratch, per dev
 
 // Device address of the scratch array on the current device.  Host code
 // cannot use the symbol itself (on the host it names a host-side stand-in),
-// so the address is looked up once per device with that device current.
+// so the address is looked up once per device with that device current and
+// kept for the life of the process (a device reset through this library's
+// runtime would invalidate it; the entry point's contract excludes that).
 static unsigned char *static_scratch(int device)
 {
     if (device < 0 || device >= kMaxDevices) raise(KD_ENODEV, "device index out of range");
@@ -1260,15 +1262,13 @@ __global__ void k_static_batch(const long long *off, int nb, int b0, long long c
 }
 
 // hist[e][qf][tf] -> out[k][qf*Fq + tf]: the pairs with d2 < rsq of radius k
-// (cumulative over sorted edges), in the reference's counter layout
+// (cumulative over sorted edges), in the reference's counter layout.  out is
+// zeroed on the stream before the launch (several (qf, tf) can share a slot
+// of that layout, so the slots are accumulated atomically): any grid works.
 __global__ void k_static_out(const unsigned long long *H, int ne, int Fqe, int Fte,
                              const int *edge_of, int nradii, int Fq, int Ft, long long *out)
 {
     const int nrow = Fq * Ft;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nradii * nrow;
-         i += gridDim.x * blockDim.x)
-        out[i] = 0;
-    __syncthreads();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nradii * Fqe * Fte;
          i += gridDim.x * blockDim.x) {
         const int k = i / (Fqe * Fte), qf = (i / Fte) % Fqe, tf = i % Fte;
@@ -1398,7 +1398,9 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
         KD_LAUNCH_CHECK("k_tiles");
         b0 = b1;
     }
-    k_static_out<<<1, 1024, 0, s>>>(H, ne, Fqe, Fte, eo, nradii, Fq, Ft, out);
+    check(cudaMemsetAsync(out, 0, sizeof(long long) * (size_t)nradii * Fq * Ft, s), "memset");
+    k_static_out<<<blocks_for((long long)nradii * Fqe * Fte, 256), 256, 0, s>>>(H, ne, Fqe, Fte, eo,
+                                                                                 nradii, Fq, Ft, out);
     KD_LAUNCH_CHECK("k_static_out");
     int herr = 0;
     check(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");

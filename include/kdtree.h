@@ -144,8 +144,10 @@ void kd_free_counts(long long *counts);
  * input points, duplicates included, each with its own field): for every
  * radius k, out[k*Fq*Ft + qf*Fq + tf] is what pair_count(tree,
  * query_points, query_fields, n, Fq, radii[k], .) returns, with
- * Fq = query.num_fields and Ft = tree.num_fields.  All radii are counted in
- * one pass over the node pairs.  Replaces the per-edge pair_count loop of
+ * Fq = query.num_fields and Ft = tree.num_fields.  Any number of radii, in
+ * any order, repeats and NaN included: up to 64 distinct squared radii are
+ * counted in one pass over the node pairs, more in passes of 64 over the
+ * same trees.  Replaces the per-edge pair_count loop of
  * clustering.py:218-230, :256-284.  mode: KD_MODE_MIXED or KD_MODE_FP64.
  * stats may be NULL.  Returns 0 or a negative error code. */
 int kd_count_radii(kdtree_t tree, kdtree_t query, const double *radii,
@@ -208,9 +210,12 @@ int kd_count_batch_shard(const kdtree_t *trees, const kdtree_t *queries, int njo
  * tile records must fit (a clear error otherwise); larger jobs run in more
  * batches, so this is slower than kd_count_radii.  The first call on a
  * device looks up the array's device address (keep that first call outside
- * any stream capture).  All calls share the array and its contents persist
- * between calls; each call clears what it needs, but calls that overlap on
- * the same GPU (other threads) race and must be serialised by the caller. */
+ * any stream capture) and keeps it for the life of the process: a caller
+ * that resets the device (cudaDeviceReset through this library's runtime)
+ * must not call this entry point afterwards.  All calls share the array and
+ * its contents persist between calls; each call clears what it needs, but
+ * calls that overlap on the same GPU (other threads) race and must be
+ * serialised by the caller. */
 int kd_count_radii_static(kdtree_t tree, kdtree_t query, const double *radii,
                           int nradii, int mode, long long *out);
 

@@ -549,6 +549,123 @@ int or_brute_counts(const or_tree_t *t, const double *q, const int *qfields,
     return OR_OK;
 }
 
+/* Bin index of d2 among the sorted squared radii: the first with d2 < rsq
+ * (nsorted when none; NaN never counts). */
+static inline int bin_of(const work_t *w, double d2)
+{
+    int lo = 0, hi = w->nsorted;
+    if (d2 != d2) return w->nsorted;
+    while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (d2 < w->rsq_sorted[mid]) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+/* The reference traversal (radius, kdquery.c:62-113) at radius w->rad, the
+ * largest of the radii, binning every visited node's distance into all the
+ * sorted radii at once.  The reference's prune at that radius never drops a
+ * pair closer than it (if fl(q + rad) < split then every point of the right
+ * subtree has fl(t - q) >= rad and so fl(d2) >= fl(rad*rad)), hence never one
+ * closer than any smaller radius: the result is the exhaustive count. */
+static void tree_bin_rec(work_t *w, int p, const double *q, int qf, int nrow)
+{
+    const or_tree_t *t = w->t;
+    int u = t->npoint[p];
+    const double *v = t->u + 3 * (size_t)u;
+    double n2 = dist2_ref(v, q);
+    w->hist[(size_t)bin_of(w, n2) * nrow + qf * w->fq + t->ufield[u]] += t->uweight[u];
+    if (!t->nhas_l[p]) return;
+    if (!t->nhas_r[p]) {
+        tree_bin_rec(w, 2 * p, q, qf, nrow);
+        return;
+    }
+    int d = t->ndim[p];
+    double val = q[d];
+    double upper = val + w->rad, lower = val - w->rad, point = v[d];
+    if (upper < point) {
+        tree_bin_rec(w, 2 * p, q, qf, nrow);
+    } else if (lower > point) {
+        tree_bin_rec(w, 2 * p + 1, q, qf, nrow);
+    } else {
+        tree_bin_rec(w, 2 * p, q, qf, nrow);
+        tree_bin_rec(w, 2 * p + 1, q, qf, nrow);
+    }
+}
+
+static void *tree_bin_worker(void *arg)
+{
+    work_t *w = (work_t *)arg;
+    int nrow = w->fq * w->t->num_fields;
+    for (int i = w->lo; i < w->hi; i++)
+        tree_bin_rec(w, 1, w->q + 3 * (size_t)i, w->qf ? w->qf[i] : 0, nrow);
+    return NULL;
+}
+
+int or_tree_counts(const or_tree_t *t, const double *q, const int *qfields,
+                   int nq, int num_fields_q, const double *radii, int nradii,
+                   int nthreads, long long *out)
+{
+    int nrow = num_fields_q * t->num_fields;
+    double rmax = 0.0;
+    if (nq < 0 || nradii < 0) return fail(OR_EINVAL, "negative size");
+    for (int k = 0; k < nradii; k++) {
+        double v = radii[k] * radii[k];
+        if (radii[k] < 0) return fail(OR_EINVAL, "negative radius");
+        if (v != v) continue;
+        /* a squared radius of +inf counts every pair: no traversal prunes */
+        if (v == INFINITY)
+            return or_brute_counts(t, q, qfields, nq, num_fields_q, radii, nradii, nthreads, out);
+        if (radii[k] > rmax) rmax = radii[k];
+    }
+    if (check_layout(t, qfields, nq, num_fields_q, nrow))
+        return fail(OR_EFIELD, "field ids overflow the reference counter layout");
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 64) nthreads = 64;
+    double *rs = (double *)malloc(sizeof(double) * (size_t)(nradii + 1));
+    int ns = 0;
+    if (!rs) return fail(OR_ENOMEM, "oom");
+    for (int k = 0; k < nradii; k++) {
+        double v = radii[k] * radii[k];
+        if (v == v) rs[ns++] = v;
+    }
+    qsort(rs, (size_t)ns, sizeof(double), cmp_dbl);
+    size_t hsz = (size_t)(ns + 1) * (size_t)nrow;
+    long long *hist = (long long *)calloc((size_t)nthreads * hsz, sizeof(long long));
+    if (!hist) { free(rs); return fail(OR_ENOMEM, "oom"); }
+    work_t ws[64];
+    for (int i = 0; i < nthreads; i++) {
+        memset(&ws[i], 0, sizeof ws[i]);
+        ws[i].t = t; ws[i].q = q; ws[i].qf = qfields; ws[i].fq = num_fields_q;
+        ws[i].lo = (int)((long long)nq * i / nthreads);
+        ws[i].hi = (int)((long long)nq * (i + 1) / nthreads);
+        ws[i].rad = rmax;
+        ws[i].rsq_sorted = rs; ws[i].nsorted = ns;
+        ws[i].hist = hist + (size_t)i * hsz;
+    }
+    if (t->n > 0) run_threads(ws, nthreads, tree_bin_worker);
+    for (int i = 1; i < nthreads; i++)
+        for (size_t j = 0; j < hsz; j++) hist[j] += hist[(size_t)i * hsz + j];
+    for (int k = 0; k < nradii; k++) {
+        double v = radii[k] * radii[k];
+        long long *o = out + (size_t)k * nrow;
+        memset(o, 0, sizeof(long long) * (size_t)nrow);
+        if (v != v) continue;
+        int lo = 0, hi = ns;
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (rs[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        for (int b = 0; b <= lo && b < ns; b++)
+            for (int j = 0; j < nrow; j++) o[j] += hist[(size_t)b * nrow + j];
+    }
+    free(rs);
+    free(hist);
+    return OR_OK;
+}
+
 /* ------------------------------------------------------------ visit count */
 
 typedef struct {

@@ -68,6 +68,14 @@ int or_brute_counts(const or_tree_t *t, const double *q, const int *qfields,
                     int nq, int num_fields_q, const double *radii, int nradii,
                     int nthreads, long long *out);
 
+/* or_brute_counts' result from the reference traversal (kdquery.c:62-113)
+ * run at the largest finite radius, every visited node's distance binned
+ * into all radii: the same exhaustive counts, far fewer distances.  Falls
+ * back to the exhaustive loop when a squared radius is +inf. */
+int or_tree_counts(const or_tree_t *t, const double *q, const int *qfields,
+                   int nq, int num_fields_q, const double *radii, int nradii,
+                   int nthreads, long long *out);
+
 /* Node distance evaluations the reference traversal (kdquery.c:62-113)
  * performs for nq queries at radius r, over a node array given by its
  * semantic fields (memsize entries; xyz interleaved).  This is the CPU

@@ -52,6 +52,9 @@ def lib():
         L.or_brute_counts.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int), c_int,
                                       c_int, POINTER(c_double), c_int, c_int,
                                       POINTER(c_longlong)]
+        L.or_tree_counts.argtypes = [c_void_p, POINTER(c_double), POINTER(c_int), c_int,
+                                     c_int, POINTER(c_double), c_int, c_int,
+                                     POINTER(c_longlong)]
         L.or_count_visits.restype = c_longlong
         L.or_count_visits.argtypes = [POINTER(c_double)] + [POINTER(c_int)] * 3 + [
             c_int, POINTER(c_double), c_int, c_double, c_int]
@@ -139,6 +142,21 @@ class OracleTree:
             raise OracleError(lib().or_last_error().decode())
         return out
 
+    def tree_counts(self, q, qfields=None, num_fields_q=1, radii=(0.1,), nthreads=8):
+        """brute_counts' result through the reference traversal pruned at the
+        largest radius (or_tree_counts): exact, and fast enough for whole
+        catalogs of a few hundred thousand points."""
+        q = np.require(q, dtype=np.float64, requirements="AC")
+        qf = None if qfields is None else np.require(qfields, dtype=np.int32, requirements="AC")
+        radii = np.require(np.asarray(radii, dtype=np.float64), requirements="AC")
+        out = np.zeros((len(radii), num_fields_q * self.num_fields), dtype=np.int64)
+        rc = lib().or_tree_counts(self._h, _dp(q), _ip(qf), c_int(q.shape[0]),
+                                  c_int(num_fields_q), _dp(radii), c_int(len(radii)),
+                                  c_int(nthreads), out.ctypes.data_as(POINTER(c_longlong)))
+        if rc != 0:
+            raise OracleError(lib().or_last_error().decode())
+        return out
+
 
 def count_visits(nodes, q, r, nthreads=8):
     """Reference traversal node visits (its "pairs tested") over a node array
@@ -172,6 +190,16 @@ def radec2sph64(ra, dec):
     th, ph = np.empty(ra.size), np.empty(ra.size)
     lib().or_radec2sph64(_dp(ra), _dp(dec), _dp(th), _dp(ph), c_int(ra.size))
     return th, ph
+
+
+def reference_root():
+    """The reference project's checkout (its ``src/`` and ``corruscant/``),
+    read from the CORRUSCANT_REF environment variable, else the location this
+    build's checker was set up against; None when neither exists.  This is
+    the one place that names it: the build step, the golden generator and
+    the side-by-side tests all ask here."""
+    root = os.environ.get("CORRUSCANT_REF", "/root/reference")
+    return root if os.path.isdir(os.path.join(root, "src")) else None
 
 
 def ref_path():

@@ -93,7 +93,9 @@ def main():
     args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
     only = [a.split("=", 1)[1].split(",") for a in sys.argv[1:] if a.startswith("--only=")]
     parts = set(only[0]) if only else {"trees", "estimators", "coords", "alltypes"}
-    ref_root = args[0] if args else "/root/reference"
+    ref_root = args[0] if args else O.reference_root()
+    if ref_root is None:
+        sys.exit("reference checkout not found: set CORRUSCANT_REF")
     if "trees" in parts:
         make_tree_goldens(R)
     if "estimators" in parts:

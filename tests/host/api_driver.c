@@ -228,12 +228,21 @@ static void scenario_faults(void)
     kd_set_precision(KD_MODE_MIXED);
     CHECK(kd_set_device(3) < 0, "device");
     {
-        double r[65];
-        long long o65[65 * 4];
-        for (n = 0; n < 65; n++) r[n] = 0.001 * (n + 1);
-        CHECK(kd_count_radii(t, t, r, 65, 0, o65, NULL) < 0, "65 distinct radii accepted");
-        CHECK(kd_count_radii(t, t, r, 64, 0, o65, NULL) == 0, "64 distinct radii refused");
-        CHECK(kd_count_radii(t, t, (const double[]){0.1, -0.1}, 2, 0, o65, NULL) < 0, "neg");
+        /* any number of distinct radii (counted in passes of 64): 150 radii,
+         * each count equal to the same radius counted on its own */
+        double r[150];
+        long long *o150 = (long long *)malloc(sizeof(long long) * 150 * 16);
+        long long one[16];
+        for (n = 0; n < 150; n++) r[n] = 0.004 * ((n * 37) % 150 + 1);
+        CHECK(kd_count_radii(t, t, r, 150, 0, o150, NULL) == 0, "150 distinct radii refused");
+        for (n = 0; n < 150; n += 7) {
+            CHECK(kd_count_radii(t, t, r + n, 1, 0, one, NULL) == 0, "one radius");
+            CHECK(memcmp(one, o150 + (size_t)n * a.nf * a.nf, sizeof(long long) * a.nf * a.nf) == 0,
+                  "radius %d of 150 differs from its own count", n);
+        }
+        CHECK(kd_count_radii_static(t, t, r, 65, 0, o150) < 0, "static: 65 radii accepted");
+        CHECK(kd_count_radii(t, t, (const double[]){0.1, -0.1}, 2, 0, o150, NULL) < 0, "neg");
+        free(o150);
     }
     /* malformed counts and pointers are errors, never memory accesses */
     CHECK(kd_count_radii(t, t, RADII, -1, 0, out, NULL) == KD_EINVAL, "negative radius count");
@@ -351,7 +360,7 @@ static void scenario_coords(void)
 /* distinct non-NaN squared radii among the first n, or -1 if one is negative */
 static int distinct_edges(const double *r, int n)
 {
-    double u[128];
+    double u[160];
     int k, j, m = 0;
     for (k = 0; k < n; k++) {
         const double v = r[k] * r[k];
@@ -381,7 +390,7 @@ static void scenario_fuzz(void)
     long long *out = (long long *)malloc(sizeof(long long) * 8192);
     long long *want = (long long *)malloc(sizeof(long long) * 8192);
     long long *cum = (long long *)malloc(sizeof(long long) * 8192);
-    double radii[80];
+    double radii[150];
     int it, i, k, succeeded = 0, refused = 0;
     for (i = 0; i < 3; i++)
         tr[i] = tree_construct(cats[i]->xyz, cats[i]->f, cats[i]->n, cats[i]->nf);
@@ -389,7 +398,7 @@ static void scenario_fuzz(void)
     for (it = 0; it < 4000; it++) {
         const int ti = (int)(urand() * 3), qi = (int)(urand() * 3), which = (int)(urand() * 5);
         const cat_t *T = cats[ti], *Q = cats[qi];
-        const int nr = (int)(urand() * 75) - 5; /* -5 .. 69 */
+        const int nr = (int)(urand() * 145) - 5; /* -5 .. 139: past one pass of 64 */
         const int mode = urand() < 0.9 ? (int)(urand() * 2) : (int)(urand() * 7) - 3;
         const int null_r = urand() < 0.05, null_o = urand() < 0.05, bad_tree = urand() < 0.03;
         const double *R = null_r ? NULL : radii;
@@ -397,14 +406,15 @@ static void scenario_fuzz(void)
         const kdtree_t tt = bad_tree ? dead : tr[ti];
         const int Fq = Q->nf, Ft = T->nf;
         int rc, ne, expect_ok;
-        for (k = 0; k < 80; k++) {
+        for (k = 0; k < 150; k++) {
             const double u = urand();
-            radii[k] = u < 0.05 ? NAN : u < 0.08 ? INFINITY : u < 0.095 ? -0.1 : urand() * 0.5;
+            radii[k] = u < 0.05 ? NAN : u < 0.08 ? INFINITY : urand() * 0.5;
         }
+        if (urand() < 0.12) radii[(int)(urand() * (nr > 0 ? nr : 1))] = -0.1; /* one negative */
         ne = nr > 0 && !null_r ? distinct_edges(radii, nr) : 0;
         /* rules shared by every entry point */
         expect_ok = !bad_tree && nr >= 0 && (nr == 0 || (!null_r && !null_o)) &&
-                    (mode == 0 || mode == 1) && ne >= 0 && ne <= 64;
+                    (mode == 0 || mode == 1) && ne >= 0;
         memset(out, 0x5a, sizeof(long long) * 8192);
         switch (which) {
         case 0: /* kd_count_radii */

@@ -152,6 +152,11 @@ int kdg_count_batch(const kd_catalog *const *trees, const kd_catalog *const *que
         kd_set_error(KD_EINVAL, "shard %d of %d", shard, nshards);
         return KD_EINVAL;
     }
+    /* the device counter's limit: the host library splits more radii into passes */
+    if (ne < 1 || ne > KD_MAX_EDGES) {
+        kd_set_error(KD_EINVAL, "fake device: %d distinct radii in one pass", ne);
+        return KD_EINVAL;
+    }
     for (j = 0; j < njobs; j++) {
         if (shard == 0) brute_hist(trees[j], queries[j], rsq, ne, hists[j]);
         else  /* every count on shard 0 in the fake */

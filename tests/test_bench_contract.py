@@ -45,7 +45,10 @@ def test_reference_arm_line():
     cb = d["cpu_baseline"]
     assert set(cb) >= {"value", "unit", "cores", "kind", "sample"}
     assert cb["kind"] == "reference" and cb["value"] == d["value"] and cb["cores"] >= 1
-    assert d["e2e"]["value"] == d["value"] and d["e2e"]["unit"] == d["unit"]
+    # e2e: exhaustive-equivalent pairs per second of a full result, the unit
+    # of the GPU arm's e2e
+    assert d["e2e"]["unit"] == "all-pairs-equivalent pairs/s" and d["e2e"]["value"] > 0
+    assert d["e2e"]["s_per_full_result"] == d["s_per_full_result"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
 
 
@@ -82,8 +85,10 @@ def test_gpu_arm_line():
     assert r["bound"] == "fp32" and r["unit"] == "TFLOP/s" and r["peak"] > 0
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-9 and r["traffic"] > 0
     e = d["e2e"]
-    assert e["unit"] == d["unit"] and e["value"] > 0 and e["h2d_bytes_per_step"] > 0
-    assert e["d2h_bytes_per_step"] > 0 and e["value"] != d["value"]
+    assert e["unit"] == "all-pairs-equivalent pairs/s" and e["value"] > 0
+    assert e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    assert e["s_per_full_result"] > 0 and d["s_per_full_result"] > 0
+    assert d["fp64_form"]["roofline"]["peak"] > 0
     c = d["clocks"]
     assert set(c) >= {"sm_mhz", "sm_max_mhz", "reasons"}
     assert isinstance(d["gpu_launches"], int) and d["gpu_launches"] >= 3

@@ -18,10 +18,10 @@ from corruscant_b200 import clustering
 from oracle import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = "/root/reference"
+REF_ROOT = O.reference_root()
 
 pytestmark = pytest.mark.skipif(
-    not (O.ref_available() and os.path.isdir(os.path.join(REF_ROOT, "corruscant"))),
+    not (O.ref_available() and REF_ROOT and os.path.isdir(os.path.join(REF_ROOT, "corruscant"))),
     reason="reference sources or oracle/_ref absent")
 
 
