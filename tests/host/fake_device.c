@@ -132,8 +132,13 @@ static void brute_hist(const kd_catalog *tc, const kd_catalog *qc, const double 
     for (i = 0; i < qc->n_raw; i++)
         for (j = 0; j < tc->n_raw; j++) {
             const double d2 = d2_ref(tp->xyz + 3 * (size_t)j, qp->xyz + 3 * (size_t)i);
-            int e = 0;
-            while (e < ne && !(d2 < rsq[e])) e++;
+            int e = 0, hi = ne; /* first e with d2 < rsq[e] (NaN: none) */
+            if (d2 != d2) e = ne;
+            while (e < hi) {
+                const int m = (e + hi) / 2;
+                if (d2 < rsq[m]) hi = m;
+                else e = m + 1;
+            }
             if (e < ne) hist[((size_t)e * Fqe + (size_t)qp->f[i]) * Fte + (size_t)(tp->f[j] & 0xFF)]++;
         }
 }
