@@ -14,8 +14,9 @@ shapes; no dataset is involved):
   angular  2,000,000 (RA, DEC) points in RA 0-90 deg, DEC -10..60 deg uniform
            in sin DEC, half of them in Gaussian blobs (sigma 0.05 deg, tangent
            plane) around 20,000 centres; 20,000,000 uniform randoms; 16 edges
-           theta = logspace(-3, log10 2, 16) deg as chords; 100 fields (10 x 10
-           data quantiles in RA x sin DEC); DD + DR + RR
+           theta = logspace(-3, log10 2, 16) deg as chords; 100 fields
+           auto-divided from the data (corruscant_b200.fields: HEALPix pixels
+           partitioned into balanced fields, min_ratio 0.5); DD + DR + RR
   mocks    128 Neyman-Scott catalogs (N/100 parents, sigma 0.005) with sizes
            log-uniform in 20,000..500,000, one shared 5,000,000-point uniform
            random catalog; 13 edges logspace(log10 2e-3, -1, 13); 16 fields
@@ -156,22 +157,26 @@ def wl_angular(scale=1.0):
     ra_c, dec_c = _blobs(rs, nc, 50, 0.05)
     ra_d, dec_d = np.concatenate([ra_b, ra_c]), np.concatenate([dec_b, dec_c])
     ra_r, dec_r = _patch_uniform(np.random.RandomState(15), nr)
-    # 100 fields: 10 x 10 quantile cells of the data in RA x sin DEC
-    qs = np.linspace(0, 1, 11)[1:-1]
-    e_ra, e_sd = np.quantile(ra_d, qs), np.quantile(np.sin(np.radians(dec_d)), qs)
-
-    def fields(ra, dec):
-        return (10 * np.searchsorted(e_ra, ra, side="right") +
-                np.searchsorted(e_sd, np.sin(np.radians(dec)), side="right")).astype(np.int32)
+    # 100 fields auto-divided from the data as the reference's fields.template
+    # does it (HEALPix pixels of the data cut into balanced parts, Nside
+    # doubled until the smallest field holds half the average); randoms take
+    # the field of their pixel
+    import contextlib
+    from corruscant_b200 import fields as flds
+    tpl = flds.template(100, ra=ra_d, dec=dec_d)
+    with contextlib.redirect_stdout(sys.stderr):
+        f_d = tpl.create_fields(min_ratio=0.5).astype(np.int32)
+    f_r = tpl.assign_fields(ra=ra_r, dec=dec_r).astype(np.int32)
     theta = np.logspace(-3, np.log10(2.0), 16)
     return Workload(
         "angular",
         ("angular w(theta) autocorr: 2M (RA,DEC) points in RA 0-90, DEC -10..60 (uniform in "
          "sin DEC), half in Gaussian blobs (sigma 0.05 deg) around 20k centres; 20M uniform "
-         "randoms; 16 theta edges logspace(-3,log10 2) deg as chords; 100 quantile fields; "
+         "randoms; 16 theta edges logspace(-3,log10 2) deg as chords; 100 auto-divided fields "
+         "(HEALPix pixels of the data partitioned, min_ratio 0.5); "
          "a step is DD+DR+RR over all edges"),
-        {"D": (angular.cartesian(ra_d, dec_d), fields(ra_d, dec_d), 100),
-         "R": (angular.cartesian(ra_r, dec_r), fields(ra_r, dec_r), 100)},
+        {"D": (angular.cartesian(ra_d, dec_d), f_d, 100),
+         "R": (angular.cartesian(ra_r, dec_r), f_r, 100)},
         [("DD", "D", "D"), ("DR", "R", "D"), ("RR", "R", "R")],
         angular.chord(theta), "synthetic (seeded sky patch: uniform + Gaussian blobs)", 4000,
         radec={"D": (ra_d, dec_d), "R": (ra_r, dec_r)})

@@ -298,5 +298,83 @@ def coordlib():
         L.radecdist2cart64.argtypes = [POINTER(c_double)] * 4 + [c_int]
         L.radec2sph64.restype = None
         L.radec2sph64.argtypes = [POINTER(c_double)] * 4 + [c_int]
+        # field division (include/fields.h)
+        L.kd_healpix_ang2pix.restype = c_int
+        L.kd_healpix_ang2pix.argtypes = [c_int, POINTER(c_double), POINTER(c_double), c_longlong,
+                                         POINTER(c_longlong)]
+        L.kd_healpix_pix2ang.restype = c_int
+        L.kd_healpix_pix2ang.argtypes = [c_int, POINTER(c_longlong), c_longlong,
+                                         POINTER(c_double), POINTER(c_double)]
+        L.kd_healpix_edge_neighbours.restype = c_int
+        L.kd_healpix_edge_neighbours.argtypes = [c_int, POINTER(c_longlong)]
+        L.kd_healpix_corners.restype = c_int
+        L.kd_healpix_corners.argtypes = [c_int, c_longlong, POINTER(c_double)]
+        L.kd_partition_graph.restype = c_longlong
+        L.kd_partition_graph.argtypes = [c_int, POINTER(c_int), POINTER(c_int),
+                                         POINTER(c_longlong), POINTER(c_longlong), c_int,
+                                         POINTER(c_int)]
         _CO = L
     return _CO
+
+
+def _llp(a):
+    return a.ctypes.data_as(POINTER(c_longlong))
+
+
+def healpix_ang2pix(nside, theta, phi):
+    """RING pixel of each (theta, phi) (healpy.ang2pix's default scheme)."""
+    theta = np.require(np.asarray(theta, dtype=np.float64), requirements="AC")
+    phi = np.require(np.asarray(phi, dtype=np.float64), requirements="AC")
+    if theta.shape != phi.shape:
+        raise ValueError("theta and phi must have the same shape")
+    out = np.empty(theta.shape, dtype=np.int64)
+    if coordlib().kd_healpix_ang2pix(int(nside), dptr(theta), dptr(phi), theta.size,
+                                     _llp(out)) != 0:
+        raise ValueError("ang2pix: nside must be in [1, 2^20] and angles not NaN")
+    return out
+
+
+def healpix_pix2ang(nside, pix):
+    """Centres (theta, phi) of RING pixels."""
+    pix = np.require(np.asarray(pix, dtype=np.int64), requirements="AC")
+    th, ph = np.empty(pix.shape), np.empty(pix.shape)
+    if coordlib().kd_healpix_pix2ang(int(nside), _llp(pix), pix.size, dptr(th), dptr(ph)) != 0:
+        raise ValueError("pix2ang: bad nside or pixel index")
+    return th, ph
+
+
+def healpix_edge_neighbours(nside):
+    """(12 nside^2, 4) int64: the south-west, north-west, north-east and
+    south-east neighbour of every RING pixel."""
+    npix = 12 * int(nside) ** 2
+    out = np.empty((npix, 4), dtype=np.int64)
+    if coordlib().kd_healpix_edge_neighbours(int(nside), _llp(out)) != 0:
+        raise ValueError("bad nside")
+    return out
+
+
+def healpix_corners(nside, pix):
+    """(3, 4) unit vectors of the pixel's north, west, south and east corners
+    (the layout of healpy.boundaries)."""
+    out = np.empty((4, 3))
+    if coordlib().kd_healpix_corners(int(nside), int(pix), dptr(out)) != 0:
+        raise ValueError("bad nside or pixel index")
+    return out.T.copy()
+
+
+def partition_graph(nparts, xadj, adjncy, vweights, eweights):
+    """Recursive-bisection partition of a weighted graph in CSR form:
+    (edge cut, part id of every vertex)."""
+    xadj = np.require(np.asarray(xadj, dtype=np.int32), requirements="AC")
+    adjncy = np.require(np.asarray(adjncy, dtype=np.int32), requirements="AC")
+    vw = np.require(np.asarray(vweights, dtype=np.int64), requirements="AC")
+    ew = np.require(np.asarray(eweights, dtype=np.int64), requirements="AC")
+    nv = len(xadj) - 1
+    if nv < 1 or len(vw) != nv or len(ew) != len(adjncy):
+        raise ValueError("malformed graph")
+    part = np.empty(nv, dtype=np.int32)
+    cut = coordlib().kd_partition_graph(nv, iptr(xadj), iptr(adjncy), _llp(vw), _llp(ew),
+                                        int(nparts), iptr(part))
+    if cut < 0:
+        raise ValueError("malformed graph or part count")
+    return int(cut), part
