@@ -70,6 +70,50 @@ def test_traversal_equals_brute_force(golden):
             assert np.array_equal(brute[k], t.pair_count(q, qf, nf, r)), (name, r)
 
 
+def test_pruned_multi_radius_counter_equals_exhaustive(golden):
+    """or_tree_counts (the traversal at the largest radius, every visited
+    distance binned into all radii) == the exhaustive loop, on every golden
+    set, a lattice with exact on-edge pairs and radii in any order; and equal
+    to the live reference build, radius by radius."""
+    g = golden("counts.npz")
+    trees = golden_sets(golden("trees.npz"))
+    radii = np.array([0.0, 0.02, np.nan, 0.05, 0.05, 0.5, 0.1, 0.25])
+    for name in trees:
+        ts = trees[name]
+        f = none_if_empty(ts["fields"])
+        nf = int(ts["num_fields"])
+        t = O.OracleTree(ts["points"], f, nf)
+        if name + "/queries" not in g:
+            continue
+        q = g[name + "/queries"]
+        qf = none_if_empty(g[name + "/qfields"])
+        assert np.array_equal(t.tree_counts(q, qf, nf, radii, nthreads=4),
+                              t.brute_counts(q, qf, nf, radii, nthreads=4)), name
+        # the goldens' own radii (0 and inf included: +inf squared falls back
+        # to the exhaustive loop)
+        gr = g["radii"]
+        got = t.tree_counts(q, qf, nf, gr, nthreads=4)
+        assert np.array_equal(got, t.brute_counts(q, qf, nf, gr, nthreads=4)), name
+        # the reference build's counts at those radii
+        assert np.array_equal(got, g[name + "/counts"].reshape(got.shape)), name
+    rs = np.random.RandomState(5)
+    lat = rs.randint(0, 64, (6000, 3)) / 64.0
+    lat[:600] = lat[600:1200]
+    t = O.OracleTree(lat, None, 1)
+    edges = np.sqrt(np.array([1, 2, 3, 5, 9, 16, 25, 50])) / 64.0
+    assert np.array_equal(t.tree_counts(lat, None, 1, edges[::-1]),
+                          t.brute_counts(lat, None, 1, edges[::-1]))
+    if O.ref_available():
+        R = O.RefLib()
+        rt = R.build(lat, None, 1)
+        try:
+            got = t.tree_counts(lat[:500], None, 1, edges)
+            for k, r in enumerate(edges):
+                assert np.array_equal(got[k], R.pair_count(rt, lat[:500], None, 1, r, 2))
+        finally:
+            R.destroy(rt)
+
+
 def test_config1_counts_golden(golden):
     c1 = golden("config1.npz")
     assert c1["dd"].sum(axis=(1, 2)).tolist() == [12, 88, 896, 7130, 52570]
