@@ -56,6 +56,16 @@ class CountStats(Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BuildStats(Structure):
+    _fields_ = [(n, c_double) for n in ("ms_prep", "ms_dedup", "ms_argsort", "ms_levels",
+                                        "ms_layout", "ms_device", "ms_node_copy",
+                                        "ms_node_wait", "ms_total_host")] + \
+               [("levels", c_int), ("n_unique", c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 assert ctypes.sizeof(KdTree) == 64
 assert ctypes.sizeof(Node) == 40
 
@@ -114,6 +124,8 @@ def kdlib():
         L.kd_tree_permutation.argtypes = [KdTree, POINTER(c_int)]
         L.kd_set_precision.restype = c_int
         L.kd_set_precision.argtypes = [c_int]
+        L.kd_tree_build_stats.restype = c_int
+        L.kd_tree_build_stats.argtypes = [KdTree, POINTER(BuildStats)]
         L.kd_set_device.restype = c_int
         L.kd_set_device.argtypes = [c_int]
         L.kd_tree_input_size.restype = c_int
@@ -266,6 +278,14 @@ def permutation(tree):
     if kdlib().kd_tree_permutation(tree, iptr(perm)) != 0:
         raise_last()
     return perm
+
+
+def build_stats(tree):
+    """kd_tree_build_stats: where the tree's build spent its time (ms)."""
+    st = BuildStats()
+    if kdlib().kd_tree_build_stats(tree, ctypes.byref(st)) != 0:
+        raise_last()
+    return st.as_dict()
 
 
 def set_precision(mode):

@@ -17,6 +17,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <sys/mman.h>
+#include <time.h>
 
 #include "kd_internal.h"
 
@@ -80,10 +81,18 @@ static kd_handle *lookup_or_fail(const kdtree_t *t, const char *what)
 
 /* ---------------------------------------------------------------- ABI */
 
+static double now_ms(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
 kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
 {
     kdtree_t t;
     kd_handle *h;
+    double t0 = now_ms(), t1, t2;
     memset(&t, 0, sizeof t);
     clear_error();
     if (!xyz || length < 1) {
@@ -103,6 +112,7 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
         free(h);
         return t;
     }
+    t1 = now_ms();
     /* every byte is written by the copy: empty heap slots come zeroed from
      * the device (as calloc leaves them in kdbuild.c:516) */
     {
@@ -127,6 +137,10 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
         return t;
     }
     kdg_drop_nodes(&h->cat);
+    t2 = now_ms();
+    h->cat.bstats.ms_build_host = t1 - t0;
+    h->cat.bstats.ms_node_copy = t2 - t1;
+    h->cat.bstats.ms_total_host = t2 - t0;
     pthread_mutex_lock(&g_lock);
     h->next = g_handles;
     g_handles = h;
@@ -165,6 +179,20 @@ int kd_tree_permutation(kdtree_t t, int *perm)
     h = lookup_or_fail(&t, "kd_tree_permutation");
     if (!h) return KD_EINVAL;
     return kdg_copy_inorder(&h->cat, perm);
+}
+
+int kd_tree_build_stats(kdtree_t t, kd_build_stats *stats)
+{
+    kd_handle *h;
+    clear_error();
+    h = lookup_or_fail(&t, "kd_tree_build_stats");
+    if (!h) return KD_EINVAL;
+    if (!stats) {
+        kd_set_error(KD_EINVAL, "kd_tree_build_stats: NULL output");
+        return KD_EINVAL;
+    }
+    *stats = h->cat.bstats;
+    return KD_OK;
 }
 
 int kd_set_device(int device)

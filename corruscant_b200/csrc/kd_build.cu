@@ -36,6 +36,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
 #include <exception>
 #include <new>
 #include <cmath>
@@ -1022,14 +1024,34 @@ template <class T> static T read1(const T *d, cudaStream_t s)
     return v;
 }
 
+static void copy_to_pageable(void *dst, const void *src, size_t bytes);
+
+static double wall_ms()
+{
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                       int query_only, kd_catalog *cat)
+                       int query_only, kd_node_sink *sink, kd_catalog *cat)
 {
     init_device();
     Stream st;
     cudaStream_t s = st.s;
     Pool pool(s);     // temporaries
     Pool keep(s);     // catalog arrays (released to the catalog on success)
+    // phase boundaries: start, dedup, argsorts, levels, layout, end
+    cudaEvent_t ph[6] = {};
+    struct EvRelease {
+        cudaEvent_t *e;
+        ~EvRelease()
+        {
+            for (int i = 0; i < 6; i++)
+                if (e[i]) cudaEventDestroy(e[i]);
+        }
+    } ev_release{ph};
+    for (auto &e : ph) check(cudaEventCreate(&e), "cudaEventCreate");
+    check(cudaEventRecord(ph[0], s), "event");
 
     // ---- inputs
     double *xyz = pool.alloc<double>(3 * (size_t)n);
@@ -1061,6 +1083,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     double maxabs;
     memcpy(&maxabs, &hv[3], sizeof maxabs);
 
+    check(cudaEventRecord(ph[1], s), "event");
     // ---- stable lexicographic sort (LSD: z, then y, then x)
     uint64_t *ktmp = pool.alloc<uint64_t>(n), *ksrt = pool.alloc<uint64_t>(n);
     int *pa = pool.alloc<int>(n), *pb = pool.alloc<int>(n);
@@ -1104,6 +1127,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     st.sync();
     if (herr) raise(herr, "a point is repeated 256 or more times (the node weight is 8 bits)");
 
+    check(cudaEventRecord(ph[2], s), "event");
     // ---- superkey argsorts of the unique points (dedup order = superkey 0)
     int *A[3], *B[3];
     for (int d = 0; d < 3; d++) {
@@ -1118,6 +1142,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     k_gather_u64<<<grid_for(n_u), TPB, 0, s>>>(u.uky, A[2], n_u, ktmp);
     sort_pairs(pool, s, ktmp, ksrt, (const int *)A[2], A[1], n_u, 0, 64);
 
+    check(cudaEventRecord(ph[3], s), "event");
     // ---- tree
     int memsize = 2;
     {
@@ -1167,8 +1192,9 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         check(cudaMemsetAsync(pos[0], 0, sizeof(int) * (size_t)n_u, s), "memset");
         st.sync();  // the host scalars above go out of scope
     }
-    int cur = 0;
+    int cur = 0, nlevels = 0;
     for (int lev = 0; (1LL << lev) <= (long long)n_u; lev++) {
+        nlevels = lev + 1;
         long long ub64 = std::min<long long>(1LL << lev, cap);
         int ub = (int)ub64;
         unsigned gs = blocks_for(ub, TPB);
@@ -1204,6 +1230,54 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     st.sync();
     if (herr) raise(herr, "tree build exceeded an internal bound");
 
+    // The node array is final: a second thread copies it to the caller's
+    // host array (pinned staging, DMA on its own stream) while this one
+    // builds the counting layout.
+    struct NodeCopy {
+        kd_node_sink *sink = nullptr;
+        void *host = nullptr;
+        bool handed = false;
+        std::thread th;
+        int code = 0;
+        char msg[160] = "";
+        double ms = 0;
+        ~NodeCopy()
+        {
+            if (th.joinable()) th.join();
+            if (host && !handed) sink->release(host);
+        }
+    } nc;
+    if (sink) {
+        const size_t nbytes = sizeof(NodeRec) * (size_t)memsize;
+        nc.sink = sink;
+        nc.host = sink->alloc(nbytes);
+        if (!nc.host) raise(KD_ENOMEM, "out of host memory for the node array");
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        const void *src = to.nodes;
+        NodeCopy *ncp = &nc;
+        auto job = [ncp, dev, src, nbytes] {
+            const double t0 = wall_ms();
+            try {
+                check(cudaSetDevice(dev), "cudaSetDevice");
+                copy_to_pageable(ncp->host, src, nbytes);
+            } catch (const Error &e) {
+                ncp->code = e.code;
+                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %s", e.msg);
+            } catch (const std::exception &e) {
+                ncp->code = KD_EINTERNAL;
+                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %s", e.what());
+            }
+            ncp->ms = wall_ms() - t0;
+        };
+        try {
+            nc.th = std::thread(job);
+        } catch (const std::exception &) {
+            job();  // no thread to spare: copy here, before the layout
+        }
+    }
+
+    check(cudaEventRecord(ph[4], s), "event");
     // ---- counting layout
     int D = 0;
     while ((long long)KD_LEAF_TARGET << D < (long long)n_u) D++;
@@ -1334,7 +1408,29 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     k_block_fill<<<blocks_for(nbn, TPB), TPB, 0, s>>>(nbn, span, leaf_r, nblk, boff, bstart, blen);
     k_block_boxes<<<nblocks, KD_BLOCK_MAX, 0, s>>>(nblocks, bstart, blen, ro, bbox, bqf);
     KD_LAUNCH_CHECK("summary kernels");
+    check(cudaEventRecord(ph[5], s), "event");
     st.sync();
+    const double wait0 = wall_ms();
+    if (nc.th.joinable()) nc.th.join();
+    const double waited = wall_ms() - wait0;
+    if (nc.code) raise(nc.code, nc.msg);
+    kd_build_stats bs;
+    memset(&bs, 0, sizeof bs);
+    bs.ms_node_copy = nc.ms;
+    bs.ms_node_wait = waited;
+    {
+        float ms[5] = {0, 0, 0, 0, 0}, tot = 0;
+        for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ph[i], ph[i + 1]);
+        cudaEventElapsedTime(&tot, ph[0], ph[5]);
+        bs.ms_prep = ms[0];
+        bs.ms_dedup = ms[1];
+        bs.ms_argsort = ms[2];
+        bs.ms_levels = ms[3];
+        bs.ms_layout = ms[4];
+        bs.ms_device = tot;
+        bs.levels = nlevels;
+        bs.n_unique = n_u;
+    }
 
     // ---- hand the kept arrays to the catalog
     memset(cat, 0, sizeof *cat);
@@ -1348,7 +1444,14 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     cat->max_tf = hfi.max_tf;
     cat->fields_split = split;
     cat->max_abs = maxabs;
-    cat->d_nodes = keep.keep(to.nodes);
+    if (sink) {
+        // the host holds the node array; the device copy is freed with the pool
+        sink->nodes = nc.host;
+        nc.handed = true;
+        cat->d_nodes = nullptr;
+    } else {
+        cat->d_nodes = keep.keep(to.nodes);
+    }
     cat->d_inorder_rep = keep.keep(inorder_rep);
     cat->d_x = keep.keep(ro.x);
     cat->d_y = keep.keep(ro.y);
@@ -1377,19 +1480,20 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     cat->d_blk_qf = keep.keep(bqf);
     cat->d_blk_box = keep.keep(bbox);
     cat->device_bytes = keep.bytes;
+    cat->bstats = bs;
 }
 
 }  // namespace kd
 
-extern "C" int kdg_build(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                         int query_only, kd_catalog *cat)
+static int build_entry(const double *h_xyz, const int *h_fields, int n, int num_fields,
+                       int query_only, kd_node_sink *sink, kd_catalog *cat)
 {
     if (n < 1) {
         kd_set_error(KD_EINVAL, "a tree needs at least one point");
         return KD_EINVAL;
     }
     try {
-        kd::build_impl(h_xyz, h_fields, n, num_fields, query_only, cat);
+        kd::build_impl(h_xyz, h_fields, n, num_fields, query_only, sink, cat);
         return KD_OK;
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);
@@ -1401,6 +1505,23 @@ extern "C" int kdg_build(const double *h_xyz, const int *h_fields, int n, int nu
         kd_set_error(KD_EINTERNAL, "host error: %s", e.what());
         return KD_EINTERNAL;
     }
+}
+
+extern "C" int kdg_build(const double *h_xyz, const int *h_fields, int n, int num_fields,
+                         int query_only, kd_catalog *cat)
+{
+    return build_entry(h_xyz, h_fields, n, num_fields, query_only, nullptr, cat);
+}
+
+extern "C" int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fields,
+                              kd_node_sink *sink, kd_catalog *cat)
+{
+    if (!sink || !sink->alloc || !sink->release) {
+        kd_set_error(KD_EINVAL, "kdg_build_tree: no node array sink");
+        return KD_EINVAL;
+    }
+    sink->nodes = nullptr;
+    return build_entry(h_xyz, h_fields, n, num_fields, 0, sink, cat);
 }
 
 // Runs a catalog operation on the catalog's device, then restores the
@@ -1487,35 +1608,6 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
 }
 
 }  // namespace kd
-
-extern "C" int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
-{
-    OnDevice on(cat->device);
-    if (!cat->d_nodes) {
-        kd_set_error(KD_EINVAL, "node array no longer held on the device");
-        return KD_EINVAL;
-    }
-    try {
-        kd::copy_to_pageable(h_nodes, cat->d_nodes, sizeof(kd::NodeRec) * (size_t)cat->memsize);
-    } catch (const kd::Error &e) {
-        kd_set_error(e.code, "node copy: %s", e.msg);
-        return e.code;
-    } catch (const std::bad_alloc &) {
-        kd_set_error(KD_ENOMEM, "out of host memory");
-        return KD_ENOMEM;
-    } catch (const std::exception &e) {
-        kd_set_error(KD_EINTERNAL, "host error: %s", e.what());
-        return KD_EINTERNAL;
-    }
-    return KD_OK;
-}
-
-extern "C" void kdg_drop_nodes(kd_catalog *cat)
-{
-    OnDevice on(cat->device);
-    if (cat->d_nodes) cudaFree(cat->d_nodes);
-    cat->d_nodes = nullptr;
-}
 
 extern "C" int kdg_copy_inorder(const kd_catalog *cat, int *h_perm)
 {

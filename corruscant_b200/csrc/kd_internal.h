@@ -86,19 +86,30 @@ typedef struct kd_catalog {
     double *d_blk_box; /* 6 per block */
 
     size_t device_bytes;
+    kd_build_stats bstats; /* phase timings of the build */
 } kd_catalog;
 
 /* Build a catalog from host arrays (xyz interleaved (n,3), fields may be
- * NULL).  query_only: the catalog only serves as the query side of counts, so
- * a point may repeat 256 or more times (only tree nodes store an 8-bit
- * weight).  Returns KD_OK or a negative status; on failure nothing is held. */
+ * NULL) to serve as the query side of counts only: a point may repeat 256 or
+ * more times (only tree nodes store an 8-bit weight) and no node array is
+ * returned.  Returns KD_OK or a negative status; on failure nothing is held. */
 int kdg_build(const double *h_xyz, const int *h_fields, int n, int num_fields,
               int query_only, kd_catalog *cat);
-/* Release the device copy of the node array (after kdg_copy_nodes). */
-void kdg_drop_nodes(kd_catalog *cat);
 
-/* Copy the node array (memsize * 40 bytes) to host memory. */
-int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes);
+/* Where a tree build puts the reference node array (tree_construct's
+ * node_data): alloc gives host memory of the requested size (NULL when out
+ * of memory), release frees it; on success nodes holds the filled array. */
+typedef struct kd_node_sink {
+    void *(*alloc)(size_t bytes);
+    void (*release)(void *p);
+    void *nodes;
+} kd_node_sink;
+
+/* kdg_build for a tree: the node array (memsize * 40 bytes) is copied into
+ * sink's host array while the counting layout is built (the device keeps no
+ * copy of it). */
+int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fields,
+                   kd_node_sink *sink, kd_catalog *cat);
 /* Copy the in-order permutation (input index of each in-order node). */
 int kdg_copy_inorder(const kd_catalog *cat, int *h_perm);
 void kdg_free(kd_catalog *cat);

@@ -126,6 +126,27 @@ typedef struct kd_count_stats {
     int launches;              /* kernel launches of the count */
 } kd_count_stats;
 
+/* Where a tree_construct call spent its time (no counterpart in the
+ * reference): device time of the build's phases, measured with events on
+ * the build's stream, and host wall time of the whole call. */
+typedef struct kd_build_stats {
+    double ms_prep;       /* device: points to the device, keys, NaN check */
+    double ms_dedup;      /* device: lexicographic sort, duplicate classes */
+    double ms_argsort;    /* device: the two superkey orders */
+    double ms_levels;     /* device: the level-by-level tree build */
+    double ms_layout;     /* device: counting layout, runs, blocks, summaries */
+    double ms_device;     /* device: first to last event of the build */
+    double ms_node_copy;  /* host: node array to the returned host array, wall
+                           * (overlapped with the counting layout) */
+    double ms_node_wait;  /* host: how long the build then waited for that copy */
+    double ms_total_host; /* host: the whole tree_construct call, wall */
+    int levels;           /* tree levels built */
+    int n_unique;         /* unique points */
+} kd_build_stats;
+
+/* Timing of the build that made `tree`.  Returns 0 or KD_EINVAL. */
+int kd_tree_build_stats(kdtree_t tree, kd_build_stats *stats);
+
 /* Last error of the calling thread: returns its code (0 = none) and copies
  * the message into buf (may be NULL). */
 int kd_last_error(char *buf, int len);
