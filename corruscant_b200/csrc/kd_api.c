@@ -88,11 +88,29 @@ static double now_ms(void)
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
+/* host memory for a node array: large ones (1.3 GB at 20M points) in 2 MB
+ * pages where the kernel offers them, so that filling it takes a few hundred
+ * page faults instead of hundreds of thousands */
+static void *alloc_nodes(size_t nb)
+{
+    void *mem = NULL;
+    if (nb >= ((size_t)64 << 20)) {
+        if (posix_memalign(&mem, (size_t)2 << 20, nb) != 0) mem = NULL;
+        if (mem) madvise(mem, nb, MADV_HUGEPAGE);
+    } else {
+        mem = malloc(nb);
+    }
+    return mem;
+}
+
+static void release_nodes(void *p) { free(p); }
+
 kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
 {
     kdtree_t t;
     kd_handle *h;
-    double t0 = now_ms(), t1, t2;
+    kd_node_sink sink;
+    double t0 = now_ms();
     memset(&t, 0, sizeof t);
     clear_error();
     if (!xyz || length < 1) {
@@ -108,39 +126,18 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
         kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
         return t;
     }
-    if (kdg_build(xyz, fields, length, num_fields, 0, &h->cat) != KD_OK) {
+    /* every byte of the node array is written by the build's copy: empty
+     * heap slots come zeroed from the device (as calloc leaves them in
+     * kdbuild.c:516) */
+    sink.alloc = alloc_nodes;
+    sink.release = release_nodes;
+    sink.nodes = NULL;
+    if (kdg_build_tree(xyz, fields, length, num_fields, &sink, &h->cat) != KD_OK) {
         free(h);
         return t;
     }
-    t1 = now_ms();
-    /* every byte is written by the copy: empty heap slots come zeroed from
-     * the device (as calloc leaves them in kdbuild.c:516) */
-    {
-        const size_t nb = (size_t)h->cat.memsize * sizeof(node_t);
-        void *mem = NULL;
-        if (nb >= ((size_t)64 << 20)) {
-            /* large node arrays (1.3 GB at 20M points) in 2 MB pages where
-             * the kernel offers them: the copy below then takes a few hundred
-             * page faults instead of hundreds of thousands */
-            if (posix_memalign(&mem, (size_t)2 << 20, nb) != 0) mem = NULL;
-            if (mem) madvise(mem, nb, MADV_HUGEPAGE);
-        } else {
-            mem = malloc(nb);
-        }
-        h->nodes = (node_t *)mem;
-    }
-    if (!h->nodes || kdg_copy_nodes(&h->cat, h->nodes) != KD_OK) {
-        if (!h->nodes) kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
-        free(h->nodes);
-        kdg_free(&h->cat);
-        free(h);
-        return t;
-    }
-    kdg_drop_nodes(&h->cat);
-    t2 = now_ms();
-    h->cat.bstats.ms_build_host = t1 - t0;
-    h->cat.bstats.ms_node_copy = t2 - t1;
-    h->cat.bstats.ms_total_host = t2 - t0;
+    h->nodes = (node_t *)sink.nodes;
+    h->cat.bstats.ms_total_host = now_ms() - t0;
     pthread_mutex_lock(&g_lock);
     h->next = g_handles;
     g_handles = h;

@@ -1263,7 +1263,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
                 copy_to_pageable(ncp->host, src, nbytes);
             } catch (const Error &e) {
                 ncp->code = e.code;
-                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %s", e.msg);
+                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %.140s", e.msg);
             } catch (const std::exception &e) {
                 ncp->code = KD_EINTERNAL;
                 snprintf(ncp->msg, sizeof ncp->msg, "node copy: %s", e.what());

@@ -78,19 +78,26 @@ oom:
     return KD_ENOMEM;
 }
 
-void kdg_drop_nodes(kd_catalog *cat)
+int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fields,
+                   kd_node_sink *sink, kd_catalog *cat)
 {
+    int rc;
+    void *host;
+    sink->nodes = NULL;
+    rc = kdg_build(h_xyz, h_fields, n, num_fields, 0, cat);
+    if (rc != KD_OK) return rc;
+    host = sink->alloc(sizeof(node_t) * (size_t)cat->memsize);
+    if (!host || fake_fail_copy) {
+        if (host) sink->release(host);
+        kdg_free(cat);
+        rc = host ? fake_fail_copy : KD_ENOMEM;
+        kd_set_error(rc, host ? "injected node copy failure" : "out of host memory");
+        return rc;
+    }
+    memcpy(host, cat->d_nodes, sizeof(node_t) * (size_t)cat->memsize);
     free(cat->d_nodes);
     cat->d_nodes = NULL;
-}
-
-int kdg_copy_nodes(const kd_catalog *cat, void *h_nodes)
-{
-    if (fake_fail_copy) {
-        kd_set_error(fake_fail_copy, "injected node copy failure");
-        return fake_fail_copy;
-    }
-    memcpy(h_nodes, cat->d_nodes, sizeof(node_t) * (size_t)cat->memsize);
+    sink->nodes = host;
     return KD_OK;
 }
 
