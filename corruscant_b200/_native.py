@@ -50,7 +50,8 @@ class CountStats(Structure):
     _fields_ = [("pairs_tested", c_longlong), ("pairs_rechecked", c_longlong),
                 ("pairs_accepted", c_longlong), ("pairs_wide", c_longlong),
                 ("edge_pairs", c_longlong), ("warp_tiles", c_longlong), ("entries", c_longlong), ("ms_traverse", c_double), ("ms_tiles", c_double),
-                ("ms_total", c_double), ("tile_launches", c_int), ("launches", c_int)]
+                ("ms_total", c_double), ("tile_launches", c_int), ("launches", c_int),
+                ("pairs_one_bin_multifield", c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

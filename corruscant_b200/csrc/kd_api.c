@@ -227,6 +227,7 @@ static void add_stats(kd_count_stats *to, const kd_count_stats *s)
     to->ms_total += s->ms_total;
     to->tile_launches += s->tile_launches;
     to->launches += s->launches;
+    to->pairs_one_bin_multifield += s->pairs_one_bin_multifield;
 }
 
 /*

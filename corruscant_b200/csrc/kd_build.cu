@@ -32,7 +32,6 @@
 // segments come from a parallel variance with a rigorous error interval around
 // the value the reference's sequential sums produce; only when the intervals of
 // the best and another dimension overlap is the sequential computation run.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <atomic>
@@ -47,6 +46,7 @@
 #include <vector>
 
 #include "kd_cuda_util.cuh"
+#include "kd_sort.cuh"
 
 namespace kd {
 
@@ -777,10 +777,6 @@ __global__ void k_run_heads(int n, const int *__restrict__ gs, int *head)
         head[i] = ((i - gs[i]) % KD_RUN_MAX) == 0;
 }
 
-struct MaxOp {
-    __device__ __forceinline__ int operator()(int a, int b) const { return a > b ? a : b; }
-};
-
 __global__ void k_runs(int n, const unsigned *__restrict__ key, const int *__restrict__ head,
                        const int *__restrict__ rid, int nleaves, int *run_start, int *run_tf,
                        int *run_leaf, int *leaf_run)
@@ -973,34 +969,36 @@ __global__ void __launch_bounds__(KD_BLOCK_MAX) k_block_boxes(int nblocks, const
 
 // ------------------------------------------------------------ helpers
 
+// Stable radix sort of (key, value) pairs by key bits [b0, b1) and device
+// scans: the project's own (kd_sort.cuh), temporaries from the call's pool.
+// Keys are unsigned or non-negative.
 template <class K, class V>
 static void sort_pairs(Pool &pool, cudaStream_t s, const K *kin, K *kout, const V *vin, V *vout,
                        int n, int b0, int b1)
 {
-    size_t tb = 0;
-    check(cub::DeviceRadixSort::SortPairs(nullptr, tb, kin, kout, vin, vout, n, b0, b1, s),
-          "radix sort (size)");
-    char *tmp = pool.alloc<char>(tb);
-    check(cub::DeviceRadixSort::SortPairs(tmp, tb, kin, kout, vin, vout, n, b0, b1, s),
-          "radix sort");
+    char *tmp = pool.alloc<char>(sort::sort_temp_bytes<K, V>(n));
+    check(sort::sort_pairs<K, V>(tmp, kin, kout, vin, vout, n, b0, b1, s), "radix sort");
 }
 
 template <class T>
 static void excl_sum(Pool &pool, cudaStream_t s, const T *in, T *out, int n)
 {
-    size_t tb = 0;
-    check(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, s), "scan (size)");
-    char *tmp = pool.alloc<char>(tb);
-    check(cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, n, s), "scan");
+    char *tmp = pool.alloc<char>(sort::scan_temp_bytes<T>(n));
+    check(sort::scan<T, sort::SumOp, false>(tmp, in, out, n, sort::SumOp(), s), "scan");
 }
 
 template <class T>
 static void incl_sum(Pool &pool, cudaStream_t s, const T *in, T *out, int n)
 {
-    size_t tb = 0;
-    check(cub::DeviceScan::InclusiveSum(nullptr, tb, in, out, n, s), "scan (size)");
-    char *tmp = pool.alloc<char>(tb);
-    check(cub::DeviceScan::InclusiveSum(tmp, tb, in, out, n, s), "scan");
+    char *tmp = pool.alloc<char>(sort::scan_temp_bytes<T>(n));
+    check(sort::scan<T, sort::SumOp, true>(tmp, in, out, n, sort::SumOp(), s), "scan");
+}
+
+template <class T>
+static void incl_max(Pool &pool, cudaStream_t s, const T *in, T *out, int n)
+{
+    char *tmp = pool.alloc<char>(sort::scan_temp_bytes<T>(n));
+    check(sort::scan<T, sort::MaxOp, true>(tmp, in, out, n, sort::MaxOp(), s), "max scan");
 }
 
 static int bit_hi(unsigned long long v) { return v ? 64 - __builtin_clzll(v) : 0; }
@@ -1355,10 +1353,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     {
         int *gh = pool.alloc<int>(n), *gs = pool.alloc<int>(n);
         k_group_heads<<<grid_for(n), TPB, 0, s>>>(n, key, gh);
-        size_t tb = 0;
-        check(cub::DeviceScan::InclusiveScan(nullptr, tb, gh, gs, MaxOp(), n, s), "scan (size)");
-        char *tmp = pool.alloc<char>(tb);
-        check(cub::DeviceScan::InclusiveScan(tmp, tb, gh, gs, MaxOp(), n, s), "max scan");
+        incl_max(pool, s, (const int *)gh, gs, n);
         k_run_heads<<<grid_for(n), TPB, 0, s>>>(n, gs, rhead);
     }
     incl_sum(pool, s, rhead, rid, n);

@@ -29,7 +29,6 @@
 //                distance in FP64.  Per-query bin counters live in shared
 //                memory and are reduced per (own field) into the global
 //                (bin, qfield, tfield) histogram when the tree field changes.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <exception>
@@ -42,6 +41,7 @@
 #include <vector>
 
 #include "kd_cuda_util.cuh"
+#include "kd_sort.cuh"
 
 namespace kd {
 
@@ -51,6 +51,11 @@ constexpr int kQ = KD_QPL;              // query points per lane
 constexpr int kTileWarpsPerCta = 4;
 constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
+// 1: the last edge of each FP32 pass of two or more edges is decided by two
+// FP32 compares and integer adds (integer pipe) instead of a ramp (FP32 pipe)
+#ifndef KD_CMP_EDGE
+#define KD_CMP_EDGE 0
+#endif
 constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
 constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
 constexpr int kRunPerLane = KD_RUN_MAX / 32;  // staged run points per lane
@@ -190,7 +195,7 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
     int sp = 1;
     long long emitted = 0;
     const long long base = FILL ? o.off[li - g0] : 0;
-    unsigned long long acc_pairs = 0;
+    unsigned long long acc_pairs = 0, blocked_pairs = 0;
     long long guard = 4LL * T.nleaves + 64;
     while (sp > 0) {
         if (--guard < 0) {
@@ -229,6 +234,11 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
                         acc_pairs += c;
                     }
                 } else if (h >= T.nleaves) {
+                    // pairs of a node pair inside one bin that are tiled only
+                    // because a side holds several fields (a per-field accept
+                    // would take them without distances)
+                    if (FILL && whole && elo == ehi)
+                        blocked_pairs += (unsigned long long)alen * (unsigned long long)T.count[h];
                     act = 2;
                     leaf = h - T.nleaves;
                     const int r0 = T.leaf_run[leaf], r1 = T.leaf_run[leaf + 1];
@@ -292,8 +302,12 @@ __global__ void __launch_bounds__(32 * kTravWarps) k_traverse(const JobDesc *__r
     }
     if (!FILL && lane == 0) o.count[li - g0] = (int)emitted;
     if (FILL) {
-        for (int off = 16; off; off >>= 1) acc_pairs += __shfl_xor_sync(0xffffffffu, acc_pairs, off);
+        for (int off = 16; off; off >>= 1) {
+            acc_pairs += __shfl_xor_sync(0xffffffffu, acc_pairs, off);
+            blocked_pairs += __shfl_xor_sync(0xffffffffu, blocked_pairs, off);
+        }
         if (lane == 0 && acc_pairs) atomicAdd(o.accepted, acc_pairs);
+        if (lane == 0 && blocked_pairs) atomicAdd(o.accepted + 4, blocked_pairs);
     }
 }
 
@@ -334,34 +348,52 @@ __device__ __forceinline__ float fma_sat(float a, float b, float c)
     return d;
 }
 
-// FP32 pass of a lane's four queries over a staged run and K (<= 4) edges.
-// Each pair gives c = sat(a_k + s * nsl_k): exactly 0 or 1 outside the band,
-// in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals acc2 = sum c^2 bit
-// for bit when every c is 0 or 1; a band pair makes them differ by at least
-// 3/16, far above the FP32 rounding of these short sums (at most
-// 4 * KD_RUN_MAX <= 512 terms in [0, 1]: each sum is off by at most
-// 512 * 512 * 2^-24 = 1/64).
+// FP32 pass of a lane's four queries over a staged run: K ramp edges, then
+// KA (0 or 1) compare edges.
+// Ramp edges: each pair gives c = sat(a_k + s * nsl_k): exactly 0 or 1
+// outside the band, in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals
+// acc2 = sum c^2 bit for bit when every c is 0 or 1; a band pair makes them
+// differ by at least 3/16, far above the FP32 rounding of these short sums
+// (at most 4 * KD_RUN_MAX <= 512 terms in [0, 1]: each sum is off by at
+// most 512 * 512 * 2^-24 = 1/64).
+// Compare edge: s against the query's lo < hi, lo rounded down from
+// R - |q'|^2 - E and hi rounded up from R - |q'|^2 + E: s < lo proves the
+// pair inside the edge, s >= hi outside; counting both (integer adds of the
+// comparisons' all-ones masks, on the integer pipe beside the FP32 ramps)
+// gives the count when they agree, and a band pair otherwise.
 // Queries travel in pairs through the packed FP32 pipe (FFMA2/FADD2: two
 // independent round-to-nearest operations per instruction, the same values
 // as the scalar chain); the saturating ramp has no packed form and stays
 // scalar.  A staged point is (X, X, Y, Y), (Z, Z, N, N): each coordinate
 // twice, so one 16-byte shared load feeds both halves of a pair.
 // Returns a bit mask of the queries with a band pair.
-template <int K>
+__device__ __forceinline__ unsigned lt_mask(float a, float b)
+{
+    unsigned m;
+    asm("set.lt.u32.f32 %0, %1, %2;" : "=r"(m) : "f"(a), "f"(b));
+    return m;
+}
+
+template <int K, int KA>
 __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int rl,
                                              const float2 (&qx)[kQ / 2],
                                              const float2 (&qy)[kQ / 2],
                                              const float2 (&qz)[kQ / 2],
                                              const float (&a)[kQ][kPass32],
-                                             const float (&nsl)[kPass32], unsigned (&pc)[kQ / 2][4])
+                                             const float (&nsl)[kPass32],
+                                             const float (&lo)[kQ], const float (&hi)[kQ],
+                                             unsigned (&pc)[kQ / 2][4])
 {
     float2 acc[kQ / 2][K], acc2[kQ / 2];
+    unsigned clo[kQ], chi[kQ];
 #pragma unroll
     for (int h = 0; h < kQ / 2; h++) {
         acc2[h] = make_float2(0.0f, 0.0f);
 #pragma unroll
         for (int k = 0; k < K; k++) acc[h][k] = make_float2(0.0f, 0.0f);
     }
+#pragma unroll
+    for (int p = 0; p < kQ; p++) clo[p] = chi[p] = 0u;
     auto point = [&](const float4 xy, const float4 zn) {
         const float2 X = make_float2(xy.x, xy.y), Y = make_float2(xy.z, xy.w);
         const float2 Z = make_float2(zn.x, zn.y), N = make_float2(zn.z, zn.w);
@@ -374,6 +406,12 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
                                              fma_sat(s.y, nsl[k], a[2 * h + 1][k]));
                 acc[h][k] = __fadd2_rn(acc[h][k], c);
                 acc2[h] = __ffma2_rn(c, c, acc2[h]);
+            }
+            if (KA) {
+                clo[2 * h] -= lt_mask(s.x, lo[2 * h]);
+                chi[2 * h] -= lt_mask(s.x, hi[2 * h]);
+                clo[2 * h + 1] -= lt_mask(s.y, lo[2 * h + 1]);
+                chi[2 * h + 1] -= lt_mask(s.y, hi[2 * h + 1]);
             }
         }
     };
@@ -404,6 +442,11 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
         }
         if (tot.x != acc2[h].x) band |= 1u << (2 * h);
         if (tot.y != acc2[h].y) band |= 2u << (2 * h);
+        if (KA) {
+            pc[h][K] = clo[2 * h] | (clo[2 * h + 1] << 16);
+            if (clo[2 * h] != chi[2 * h]) band |= 1u << (2 * h);
+            if (clo[2 * h + 1] != chi[2 * h + 1]) band |= 2u << (2 * h);
+        }
     }
     return band;
 }
@@ -505,6 +548,7 @@ template <int MODE> struct WarpSmem {
     JobDesc job;  // the job of the block being counted
     float Aw[KD_MAX_EDGES];
     float nsl[KD_MAX_EDGES];
+    double Ew[KD_MAX_EDGES];  // band half-width of each edge for this block
     double cmax2;  // squared leaf-centre distance below which FP32 is safe
     int uq[kMaxDistinctQf];
     float4 stage[MODE == KD_MODE_MIXED ? 2 * KD_RUN_MAX : 1];  // (X,X,Y,Y), (Z,Z,N,N)
@@ -618,9 +662,11 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     const double inv4e = 0.25 / band_halfwidth(R[k], Rq, J.hT);
                     ws->nsl[k] = (float)(-inv4e);
                     ws->Aw[k] = (float)(0.5 + R[k] * inv4e);
+                    ws->Ew[k] = 0.25 / inv4e;
                 } else {
                     ws->nsl[k] = 0.0f;
                     ws->Aw[k] = 0.0f;
+                    ws->Ew[k] = 0.0;
                 }
             }
         }
@@ -779,20 +825,45 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     for (int k = 0; k < 4; k++) pc[h][k] = 0;
                 unsigned redo = vmask;
                 if (fp32) {
-                    float a[kQ][kPass32], sl[kPass32];
+                    // the pass's last edge by compares when it has two or
+                    // more (KD_CMP_EDGE), the others by ramps
+                    const int kr = (KD_CMP_EDGE && kn >= 2) ? kn - 1 : kn;
+                    float a[kQ][kPass32], sl[kPass32], lo[kQ], hi[kQ];
 #pragma unroll
                     for (int k = 0; k < kPass32; k++) {
-                        sl[k] = k < kn ? ws->nsl[k0 + kb + k] : 0.0f;
-                        const float Ak = k < kn ? ws->Aw[k0 + kb + k] : 0.0f;
+                        sl[k] = k < kr ? ws->nsl[k0 + kb + k] : 0.0f;
+                        const float Ak = k < kr ? ws->Aw[k0 + kb + k] : 0.0f;
 #pragma unroll
                         for (int p = 0; p < kQ; p++) a[p][k] = fmaf(qn[p], sl[k], Ak);
                     }
+#pragma unroll
+                    for (int p = 0; p < kQ; p++) lo[p] = hi[p] = 0.0f;
+                    if (KD_CMP_EDGE && kn >= 2) {
+                        const double Rc = R[k0 + kb + kr], Ec = ws->Ew[k0 + kb + kr];
+#pragma unroll
+                        for (int p = 0; p < kQ; p++) {
+                            // |q'|^2 exactly enough (FP32 squares are exact in FP64)
+                            const double q2 = (double)qx[p] * qx[p] + (double)qy[p] * qy[p] +
+                                              (double)qz[p] * qz[p];
+                            lo[p] = __double2float_rd((Rc - q2) - Ec);
+                            hi[p] = __double2float_ru((Rc - q2) + Ec);
+                        }
+                    }
                     unsigned band;
-                    switch (kn) {
-                    case 1: band = fp32_run<1>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
-                    case 2: band = fp32_run<2>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
-                    case 3: band = fp32_run<3>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
-                    default: band = fp32_run<4>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    if (!KD_CMP_EDGE) {
+                        switch (kn) {
+                        case 1: band = fp32_run<1, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        case 2: band = fp32_run<2, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        case 3: band = fp32_run<3, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        default: band = fp32_run<4, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        }
+                    } else {
+                        switch (kn) {
+                        case 1: band = fp32_run<1, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        case 2: band = fp32_run<1, 1>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        case 3: band = fp32_run<2, 1>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        default: band = fp32_run<3, 1>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
+                        }
                     }
                     redo = band & vmask;
                     rechecked += (unsigned long long)__popc(redo) * rl;
@@ -1186,6 +1257,7 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
         stats->pairs_tested = (long long)hs[0];
         stats->pairs_rechecked = (long long)hs[1];
         stats->pairs_accepted = (long long)hs[2];
+        stats->pairs_one_bin_multifield = (long long)hs[6];
         stats->pairs_wide = (long long)hs[3];
         stats->edge_pairs = (long long)hs[4];
         stats->warp_tiles = (long long)hs[5];
@@ -1319,8 +1391,7 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
     auto *out = (long long *)take(sizeof(long long) * (size_t)nradii * Fq * Ft);
     auto *cnt = (long long *)take(sizeof(long long) * ((size_t)nb + 1));
     auto *off = (long long *)take(sizeof(long long) * ((size_t)nb + 1));
-    size_t scan_bytes = 0;
-    check(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, cnt, off, nb + 1, s), "scan size");
+    const size_t scan_bytes = sort::scan_temp_bytes<long long>(nb + 1);
     void *scan_tmp = take(scan_bytes);
     const int rel_cap = 4096;  // blocks per batch
     auto *rel = (long long *)take(sizeof(long long) * (rel_cap + 1));
@@ -1352,7 +1423,8 @@ static void count_static_impl(const kd_catalog *tc, int Ft, const kd_catalog *qc
                                                                                   ne, 0, nb, to);
     KD_LAUNCH_CHECK("k_traverse(count)");
     k_gather_widen<<<blocks_for(nb, 256), 256, 0, s>>>((const int *)off, nb, cnt);
-    check(cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, cnt, off, nb + 1, s), "scan");
+    check(sort::scan<long long, sort::SumOp, false>(scan_tmp, cnt, off, nb + 1, sort::SumOp(), s),
+          "scan");
 
     const size_t smem = tile_smem(ne, mode);
     auto kern = mode == KD_MODE_MIXED ? k_tiles<KD_MODE_MIXED> : k_tiles<KD_MODE_FP64>;

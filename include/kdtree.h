@@ -124,6 +124,8 @@ typedef struct kd_count_stats {
     double ms_total;           /* device time: whole count */
     int tile_launches;
     int launches;              /* kernel launches of the count */
+    long long pairs_one_bin_multifield; /* tested pairs of node pairs lying inside one
+                                         * bin, tiled because a side holds several fields */
 } kd_count_stats;
 
 /* Where a tree_construct call spent its time (no counterpart in the
