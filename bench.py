@@ -607,10 +607,12 @@ def _summary(w, m, steps, peak, peak64, D):
     }
 
 
-def _config(w, D):
+def _config(w, world):
+    """The workload description both arms print (identical for the same
+    workload and rank count)."""
     sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
     cfg = {"workload": w.description, "counts": len(w.jobs), "edges": len(w.radii),
-           "parallelism": f"query blocks sharded over {D.world} GPU(s)",
+           "parallelism": f"{world} rank(s): query blocks sharded over the GPUs",
            "l2": "inputs larger than L2 (tree points stream from HBM each step)"}
     if len(sizes) <= 4:
         cfg["catalogs"] = sizes
@@ -637,7 +639,7 @@ def run_mine(args):
         line = {"metric": METRIC, "unit": UNIT, "n_gpus": D.world, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "f32+f64", "data": w.data,
-                "config": _config(w, D)}
+                "config": _config(w, D.world)}
         line.update(_summary(w, m, args.steps, peak, peak64, D))
         line = {k: line[k] for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup",
                                      "ms_per_step")} | line
@@ -657,7 +659,7 @@ def run_mine(args):
             wo = WORKLOADS[name](1.0)
             mo = _measure(N, D, wo, OTHER_STEPS, 3)
             o = _summary(wo, mo, OTHER_STEPS, peak, peak64, D)
-            o = {"config": _config(wo, D), "steps": OTHER_STEPS, "warmup": 3} | {
+            o = {"config": _config(wo, D.world), "steps": OTHER_STEPS, "warmup": 3} | {
                 k: o[k] for k in ("value", "ms_per_step", "s_per_full_result", "fp64_form",
                                   "mixed_over_fp64", "counts_exact_mixed_vs_fp64", "recheck_rate",
                                   "all_pairs_equivalent_per_s", "roofline", "fp32_pipe_model",
@@ -786,12 +788,7 @@ def run_reference(args):
     if cb.get("value") is None:
         print(json.dumps({"impl": "reference", "unavailable": cb.get("unavailable")}))
         return
-    sizes = {k: len(v[0]) for k, v in w.catalogs.items()}
-    cfg = {"workload": w.description, "counts": len(w.jobs), "edges": len(w.radii)}
-    if len(sizes) <= 4:
-        cfg["catalogs"] = sizes
-    else:
-        cfg["catalogs"] = len(sizes)
+    cfg = _config(w, int(os.environ.get("WORLD_SIZE", "1")))
     full_s = cb["full_result_s_extrapolated"]
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,

@@ -50,6 +50,9 @@ def test_reference_arm_line():
     assert d["e2e"]["unit"] == "all-pairs-equivalent pairs/s" and d["e2e"]["value"] > 0
     assert d["e2e"]["s_per_full_result"] == d["s_per_full_result"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # the same config object the GPU arm prints for this workload and rank count
+    import bench
+    assert d["config"] == bench._config(bench.WORKLOADS["clustered3d"](0.01), 1)
 
 
 @pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built")

@@ -74,3 +74,26 @@ def test_angular_autocorr_matches_oracle():
     assert np.array_equal(res.dd, dd)
     assert np.array_equal(res.rr, rr)
     assert res.radii_units == "degrees"
+
+
+def test_build_statistics_and_overlapped_node_copy():
+    """kd_tree_build_stats: every device phase timed, the node array copied
+    while the layout was built; the copied array is the oracle's."""
+    rs = np.random.RandomState(8)
+    p = rs.rand(300_000, 3)
+    f = (p[:, 0] * 4).astype(np.int32)
+    t = _native.build_tree(p, f, 4)
+    try:
+        st = _native.build_stats(t)
+        for k in ("ms_prep", "ms_dedup", "ms_argsort", "ms_levels", "ms_layout", "ms_device",
+                  "ms_node_copy", "ms_total_host"):
+            assert st[k] > 0, k
+        assert st["ms_node_wait"] >= 0 and st["n_unique"] == 300_000 and st["levels"] >= 18
+        parts = sum(st[k] for k in ("ms_prep", "ms_dedup", "ms_argsort", "ms_levels",
+                                    "ms_layout"))
+        assert abs(parts - st["ms_device"]) < 0.01 * st["ms_device"] + 0.05
+        nodes, onodes = _native.node_fields(t), O.OracleTree(p, f, 4).nodes()
+        for k in nodes:
+            assert np.array_equal(nodes[k], onodes[k]), k
+    finally:
+        _native.destroy(t)
