@@ -512,6 +512,13 @@ def _measure(N, D, w, steps, warmup):
         dt = time.perf_counter() - t0
         d2h = 40 * sum(t.memsize for t in tt.values()) + 8 * len(radii) * sum(
             tt[t].num_fields * tt[q].num_fields for _, t, q in w.jobs)
+        if len(tt) <= 4:  # where the builds of the last step spent their time
+            bstats = {k: {f: round(v, 3) if isinstance(v, float) else v
+                          for f, v in N.build_stats(t).items()} for k, t in tt.items()}
+        else:
+            bstats = {"catalogs": len(tt), "ms_total_host_sum": round(sum(
+                N.build_stats(t)["ms_total_host"] for t in tt.values()), 3)}
+        count_s = s["ms_total"] * 1e-3
         for t in tt.values():
             N.destroy(t)
         if it > 0:  # the first iteration warms the allocator
@@ -527,7 +534,8 @@ def _measure(N, D, w, steps, warmup):
         e_wall=float(D.reduce([e2e_wall], "MAX")[0]),
         e_pairs=int(D.reduce([e2e_pairs], "SUM")[0]),
         rechecked=int(D.reduce([mixed["rechecked"]], "SUM")[0]),
-        h2d=int(h2d), d2h=int(d2h), pinned=host is not None)
+        h2d=int(h2d), d2h=int(d2h), pinned=host is not None, build_stats=bstats,
+        e2e_count_s=count_s)
 
 
 def _fp64_lane_peak(device, mhz):
@@ -601,7 +609,9 @@ def _summary(w, m, steps, peak, peak64, D):
                 "h2d_bytes_per_step": m["h2d"], "d2h_bytes_per_step": m["d2h"],
                 "s_per_step": e_s, "s_per_full_result": e_s,
                 "pairs_tested_per_s": m["e_pairs"] / m["e_wall"],
-                "host_buffers": "pinned" if m["pinned"] else "pageable"},
+                "host_buffers": "pinned" if m["pinned"] else "pageable",
+                "count_device_s_last_step": m["e2e_count_s"],
+                "build_stats_last_step": m["build_stats"]},
         "clocks": m["clocks"],
         "gpu_launches": int(mixed["launches"]),
     }
