@@ -51,11 +51,6 @@ constexpr int kQ = KD_QPL;              // query points per lane
 constexpr int kTileWarpsPerCta = 4;
 constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
-// 1: the last edge of each FP32 pass of two or more edges is decided by two
-// FP32 compares and integer adds (integer pipe) instead of a ramp (FP32 pipe)
-#ifndef KD_CMP_EDGE
-#define KD_CMP_EDGE 0
-#endif
 // 1: in mixed mode, a record is counted together with the next one of its
 // block when both have the same tree field, edge window and histogram and
 // their runs fit 2 * KD_RUN_MAX staged points (one pass, one epilogue)
@@ -355,52 +350,35 @@ __device__ __forceinline__ float fma_sat(float a, float b, float c)
     return d;
 }
 
-// FP32 pass of a lane's four queries over a staged run: K ramp edges, then
-// KA (0 or 1) compare edges.
-// Ramp edges: each pair gives c = sat(a_k + s * nsl_k): exactly 0 or 1
-// outside the band, in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals
-// acc2 = sum c^2 bit for bit when every c is 0 or 1; a band pair makes them
-// differ by at least 3/16, far above the FP32 rounding of these short sums
-// (at most 4 * KD_RUN_MAX <= 512 terms in [0, 1]: each sum is off by at
-// most 512 * 512 * 2^-24 = 1/64).
-// Compare edge: s against the query's lo < hi, lo rounded down from
-// R - |q'|^2 - E and hi rounded up from R - |q'|^2 + E: s < lo proves the
-// pair inside the edge, s >= hi outside; counting both (integer adds of the
-// comparisons' all-ones masks, on the integer pipe beside the FP32 ramps)
-// gives the count when they agree, and a band pair otherwise.
+// FP32 pass of a lane's four queries over a staged run and K (<= 4) edges.
+// Each pair gives c = sat(a_k + s * nsl_k): exactly 0 or 1 outside the band,
+// in [1/4, 3/4] inside it.  Per query, sum_k acc_k equals acc2 = sum c^2 bit
+// for bit when every c is 0 or 1; a band pair makes them differ by at least
+// 3/16, far above the FP32 rounding of these short sums (at most
+// 4 * kStageMax <= 512 terms in [0, 1]: each sum is off by at most
+// 512 * 512 * 2^-24 = 1/64).
 // Queries travel in pairs through the packed FP32 pipe (FFMA2/FADD2: two
 // independent round-to-nearest operations per instruction, the same values
 // as the scalar chain); the saturating ramp has no packed form and stays
 // scalar.  A staged point is (X, X, Y, Y), (Z, Z, N, N): each coordinate
 // twice, so one 16-byte shared load feeds both halves of a pair.
 // Returns a bit mask of the queries with a band pair.
-__device__ __forceinline__ unsigned lt_mask(float a, float b)
-{
-    unsigned m;
-    asm("set.lt.u32.f32 %0, %1, %2;" : "=r"(m) : "f"(a), "f"(b));
-    return m;
-}
-
-template <int K, int KA>
+template <int K>
 __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int rl,
                                              const float2 (&qx)[kQ / 2],
                                              const float2 (&qy)[kQ / 2],
                                              const float2 (&qz)[kQ / 2],
                                              const float (&a)[kQ][kPass32],
                                              const float (&nsl)[kPass32],
-                                             const float (&lo)[kQ], const float (&hi)[kQ],
                                              unsigned (&pc)[kQ / 2][4])
 {
     float2 acc[kQ / 2][K], acc2[kQ / 2];
-    unsigned clo[kQ], chi[kQ];
 #pragma unroll
     for (int h = 0; h < kQ / 2; h++) {
         acc2[h] = make_float2(0.0f, 0.0f);
 #pragma unroll
         for (int k = 0; k < K; k++) acc[h][k] = make_float2(0.0f, 0.0f);
     }
-#pragma unroll
-    for (int p = 0; p < kQ; p++) clo[p] = chi[p] = 0u;
     auto point = [&](const float4 xy, const float4 zn) {
         const float2 X = make_float2(xy.x, xy.y), Y = make_float2(xy.z, xy.w);
         const float2 Z = make_float2(zn.x, zn.y), N = make_float2(zn.z, zn.w);
@@ -413,12 +391,6 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
                                              fma_sat(s.y, nsl[k], a[2 * h + 1][k]));
                 acc[h][k] = __fadd2_rn(acc[h][k], c);
                 acc2[h] = __ffma2_rn(c, c, acc2[h]);
-            }
-            if (KA) {
-                clo[2 * h] -= lt_mask(s.x, lo[2 * h]);
-                chi[2 * h] -= lt_mask(s.x, hi[2 * h]);
-                clo[2 * h + 1] -= lt_mask(s.y, lo[2 * h + 1]);
-                chi[2 * h + 1] -= lt_mask(s.y, hi[2 * h + 1]);
             }
         }
     };
@@ -449,11 +421,6 @@ __device__ __forceinline__ unsigned fp32_run(const float4 *__restrict__ ts, int 
         }
         if (tot.x != acc2[h].x) band |= 1u << (2 * h);
         if (tot.y != acc2[h].y) band |= 2u << (2 * h);
-        if (KA) {
-            pc[h][K] = clo[2 * h] | (clo[2 * h + 1] << 16);
-            if (clo[2 * h] != chi[2 * h]) band |= 1u << (2 * h);
-            if (clo[2 * h + 1] != chi[2 * h + 1]) band |= 2u << (2 * h);
-        }
     }
     return band;
 }
@@ -560,7 +527,6 @@ template <int MODE> struct WarpSmem {
     JobDesc job;  // the job of the block being counted
     float Aw[KD_MAX_EDGES];
     float nsl[KD_MAX_EDGES];
-    double Ew[KD_MAX_EDGES];  // band half-width of each edge for this block
     double cmax2;  // squared leaf-centre distance below which FP32 is safe
     int uq[kMaxDistinctQf];
     float4 stage[MODE == KD_MODE_MIXED ? 2 * kStageMax : 1];  // (X,X,Y,Y), (Z,Z,N,N)
@@ -674,11 +640,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     const double inv4e = 0.25 / band_halfwidth(R[k], Rq, J.hT);
                     ws->nsl[k] = (float)(-inv4e);
                     ws->Aw[k] = (float)(0.5 + R[k] * inv4e);
-                    ws->Ew[k] = 0.25 / inv4e;
                 } else {
                     ws->nsl[k] = 0.0f;
                     ws->Aw[k] = 0.0f;
-                    ws->Ew[k] = 0.0;
                 }
             }
         }
@@ -864,45 +828,20 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     for (int k = 0; k < 4; k++) pc[h][k] = 0;
                 unsigned redo = vmask;
                 if (fp32) {
-                    // the pass's last edge by compares when it has two or
-                    // more (KD_CMP_EDGE), the others by ramps
-                    const int kr = (KD_CMP_EDGE && kn >= 2) ? kn - 1 : kn;
-                    float a[kQ][kPass32], sl[kPass32], lo[kQ], hi[kQ];
+                    float a[kQ][kPass32], sl[kPass32];
 #pragma unroll
                     for (int k = 0; k < kPass32; k++) {
-                        sl[k] = k < kr ? ws->nsl[k0 + kb + k] : 0.0f;
-                        const float Ak = k < kr ? ws->Aw[k0 + kb + k] : 0.0f;
+                        sl[k] = k < kn ? ws->nsl[k0 + kb + k] : 0.0f;
+                        const float Ak = k < kn ? ws->Aw[k0 + kb + k] : 0.0f;
 #pragma unroll
                         for (int p = 0; p < kQ; p++) a[p][k] = fmaf(qn[p], sl[k], Ak);
                     }
-#pragma unroll
-                    for (int p = 0; p < kQ; p++) lo[p] = hi[p] = 0.0f;
-                    if (KD_CMP_EDGE && kn >= 2) {
-                        const double Rc = R[k0 + kb + kr], Ec = ws->Ew[k0 + kb + kr];
-#pragma unroll
-                        for (int p = 0; p < kQ; p++) {
-                            // |q'|^2 exactly enough (FP32 squares are exact in FP64)
-                            const double q2 = (double)qx[p] * qx[p] + (double)qy[p] * qy[p] +
-                                              (double)qz[p] * qz[p];
-                            lo[p] = __double2float_rd((Rc - q2) - Ec);
-                            hi[p] = __double2float_ru((Rc - q2) + Ec);
-                        }
-                    }
                     unsigned band;
-                    if (!KD_CMP_EDGE) {
-                        switch (kn) {
-                        case 1: band = fp32_run<1, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        case 2: band = fp32_run<2, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        case 3: band = fp32_run<3, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        default: band = fp32_run<4, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        }
-                    } else {
-                        switch (kn) {
-                        case 1: band = fp32_run<1, 0>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        case 2: band = fp32_run<1, 1>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        case 3: band = fp32_run<2, 1>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        default: band = fp32_run<3, 1>(ws->stage, rl, qx2, qy2, qz2, a, sl, lo, hi, pc); break;
-                        }
+                    switch (kn) {
+                    case 1: band = fp32_run<1>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    case 2: band = fp32_run<2>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    case 3: band = fp32_run<3>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
+                    default: band = fp32_run<4>(ws->stage, rl, qx2, qy2, qz2, a, sl, pc); break;
                     }
                     redo = band & vmask;
                     rechecked += (unsigned long long)__popc(redo) * rl;

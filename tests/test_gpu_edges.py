@@ -16,7 +16,7 @@ def _clustered(rs, n, nparents, sigma):
     return (c[rs.randint(0, nparents, n)] + rs.normal(0, sigma, (n, 3))) % 1.0
 
 
-def test_64_distinct_edges_and_no_more():
+def test_64_distinct_edges_in_one_pass_65_in_two():
     rs = np.random.RandomState(41)
     p = rs.rand(20000, 3)
     t = N.build_tree(p, None, 1)
@@ -28,8 +28,11 @@ def test_64_distinct_edges_and_no_more():
         # repeated radii do not count toward the limit and get the same rows
         rep = np.concatenate([radii, radii[::7]])
         assert np.array_equal(N.count_radii(t, t, rep), np.concatenate([want, want[::7]]))
-        with pytest.raises(N.NativeError):
-            N.count_radii(t, t, np.linspace(0.001, 0.2, 65))
+        # a 65th distinct radius takes a second pass over the trees
+        r65 = np.linspace(0.001, 0.2, 65)
+        got, st = N.count_radii(t, t, r65, with_stats=True)
+        assert np.array_equal(got, O.OracleTree(p).brute_counts(p, None, 1, r65, nthreads=8))
+        assert st["tile_launches"] >= 2
     finally:
         N.destroy(t)
 
