@@ -467,7 +467,7 @@ def _measure(N, D, w, steps, warmup):
             step(mode)
         D.barrier()
         acc = dict(dev_ms=0.0, pairs=0, launches=0, tile_launches=0, tiles_ms=0.0, rechecked=0,
-                   edge_pairs=0)
+                   edge_pairs=0, accepted=0, one_bin_multifield=0, trav_ms=0.0)
         res = None
         for _ in range(k):
             res, s = step(mode)
@@ -478,6 +478,9 @@ def _measure(N, D, w, steps, warmup):
             acc["tiles_ms"] += s["ms_tiles"]
             acc["rechecked"] += s["pairs_rechecked"]
             acc["edge_pairs"] += s["edge_pairs"]
+            acc["accepted"] += s["pairs_accepted"]
+            acc["one_bin_multifield"] += s["pairs_one_bin_multifield"]
+            acc["trav_ms"] += s["ms_traverse"]
         acc["res"] = res
         D.barrier()
         return acc
@@ -602,6 +605,14 @@ def _summary(w, m, steps, peak, peak64, D):
         "mixed_over_fp64": value / (m["fpairs"] / m["fdev_s"]),
         "counts_exact_mixed_vs_fp64": m["exact"],
         "recheck_rate": m["rechecked"] / max(1, m["pairs"]),
+        # whole node pairs inside one bin: accepted without distances (single
+        # field on both sides), and those tiled only because a side holds
+        # several fields
+        "node_pair_accepts_per_step": {
+            "pairs_accepted": mixed["accepted"] / steps,
+            "pairs_one_bin_multifield": mixed["one_bin_multifield"] / steps,
+            "pairs_tested": mixed["pairs"] / steps},
+        "traverse_ms_per_step": mixed["trav_ms"] / steps,
         "pairs_rechecked_per_step": m["rechecked"] / steps,
         "build_s": m["build_s"],
         "roofline": roofline,
@@ -673,7 +684,7 @@ def run_mine(args):
                 k: o[k] for k in ("value", "ms_per_step", "s_per_full_result", "fp64_form",
                                   "mixed_over_fp64", "counts_exact_mixed_vs_fp64", "recheck_rate",
                                   "all_pairs_equivalent_per_s", "roofline", "fp32_pipe_model",
-                                  "e2e", "clocks", "build_s")}
+                                  "node_pair_accepts_per_step", "e2e", "clocks", "build_s")}
             if not args.no_cpu_baseline:
                 cb = cpu_baseline(wo, n_queries=args.cpu_queries, gpu=N)
                 o["cpu_baseline"] = cb

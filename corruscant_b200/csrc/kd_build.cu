@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
 #include <exception>
 #include <new>
@@ -1190,6 +1191,104 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         check(cudaMemsetAsync(pos[0], 0, sizeof(int) * (size_t)n_u, s), "memset");
         st.sync();  // the host scalars above go out of scope
     }
+    // The node array goes to the caller's host array level by level while
+    // the tree is built: iteration lev of the loop below writes the heap
+    // slots of level lev (and, for segments of at most three points, their
+    // children), so once it has run, every slot below 2^(lev+1) is final.
+    // The build records an event after each iteration and queues that
+    // level's slots; a second host thread waits for each event and copies
+    // the slots (pinned staging, DMA on its own stream) while the build
+    // goes on, then the rest once the loop ends, during the counting layout.
+    struct NodeCopy {
+        kd_node_sink *sink = nullptr;
+        void *host = nullptr;
+        bool handed = false;
+        std::thread th;
+        std::mutex mu;
+        std::condition_variable cv;
+        struct Item {
+            cudaEvent_t ev;
+            size_t off, len;
+        };
+        std::vector<Item> items;
+        size_t next = 0;     // first item the copier has not taken
+        bool closed = false; // no more items
+        std::vector<cudaEvent_t> events;
+        int code = 0;
+        char msg[160] = "";
+        double ms = 0;
+        void push(cudaEvent_t ev, size_t off, size_t len)
+        {
+            std::lock_guard<std::mutex> g(mu);
+            items.push_back({ev, off, len});
+            cv.notify_one();
+        }
+        void close()
+        {
+            std::lock_guard<std::mutex> g(mu);
+            closed = true;
+            cv.notify_one();
+        }
+        ~NodeCopy()
+        {
+            close();
+            if (th.joinable()) th.join();
+            for (auto e : events) cudaEventDestroy(e);
+            if (host && !handed) sink->release(host);
+        }
+    } nc;
+    const size_t node_bytes = sizeof(NodeRec) * (size_t)memsize;
+    size_t node_queued = sizeof(NodeRec);  // slot 0 is never written: it stays zero
+    // queue the node slots [node_queued, upto) once the stream reaches here
+    auto queue_nodes = [&](size_t upto) {
+        if (!sink || upto <= node_queued) return;
+        cudaEvent_t ev = nullptr;
+        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        nc.events.push_back(ev);
+        check(cudaEventRecord(ev, s), "event");
+        nc.push(ev, node_queued, upto - node_queued);
+        node_queued = upto;
+    };
+    if (sink) {
+        nc.sink = sink;
+        nc.host = sink->alloc(node_bytes);
+        if (!nc.host) raise(KD_ENOMEM, "out of host memory for the node array");
+        memset(nc.host, 0, sizeof(NodeRec));
+        int dev = 0;
+        check(cudaGetDevice(&dev), "cudaGetDevice");
+        const char *src = (const char *)to.nodes;
+        NodeCopy *ncp = &nc;
+        auto job = [ncp, dev, src] {
+            const double t0 = wall_ms();
+            try {
+                check(cudaSetDevice(dev), "cudaSetDevice");
+                for (;;) {
+                    NodeCopy::Item it;
+                    {
+                        std::unique_lock<std::mutex> g(ncp->mu);
+                        ncp->cv.wait(g, [ncp] { return ncp->next < ncp->items.size() || ncp->closed; });
+                        if (ncp->next == ncp->items.size()) break;
+                        it = ncp->items[ncp->next++];
+                    }
+                    check(cudaEventSynchronize(it.ev), "node copy wait");
+                    copy_to_pageable((char *)ncp->host + it.off, src + it.off, it.len);
+                }
+            } catch (const Error &e) {
+                ncp->code = e.code;
+                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %.140s", e.msg);
+            } catch (const std::exception &e) {
+                ncp->code = KD_EINTERNAL;
+                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %s", e.what());
+            }
+            ncp->ms = wall_ms() - t0;
+        };
+        try {
+            nc.th = std::thread(job);
+        } catch (const std::exception &) {
+            // no thread to spare: the copy runs on this thread at the end
+        }
+    }
+
     int cur = 0, nlevels = 0;
     for (int lev = 0; (1LL << lev) <= (long long)n_u; lev++) {
         nlevels = lev + 1;
@@ -1209,6 +1308,12 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         k_level_nodes<<<gs, TPB, 0, s>>>(S, ub, lb, A[0], A[1], A[2], u, to, err);
         KD_LAUNCH_CHECK("level kernels");
         if (maxsize < 4) break;  // every segment of this level was a base case
+        // levels 0 .. lev are final: copy their slots once they are large
+        // enough to be worth a copy of their own
+        {
+            const size_t upto = sizeof(NodeRec) * std::min<size_t>((size_t)2 << lev, memsize);
+            if (upto - node_queued >= ((size_t)4 << 20)) queue_nodes(upto);
+        }
         k_mark<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, lb, A[0], A[1], A[2], side);
         for (int d = 0; d < 3; d++) {
             k_part_flags<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, A[d], side, pf);
@@ -1222,58 +1327,21 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         KD_LAUNCH_CHECK("partition kernels");
         cur ^= 1;
     }
+    // every slot is final: queue the rest and let the copier finish it while
+    // the counting layout is built
+    queue_nodes(node_bytes);
+    nc.close();
+    if (sink && !nc.th.joinable()) {  // no copier thread: copy here
+        for (auto &it : nc.items) {
+            check(cudaEventSynchronize(it.ev), "node copy wait");
+            copy_to_pageable((char *)nc.host + it.off, (const char *)to.nodes + it.off, it.len);
+        }
+    }
     int *inorder_rep = keep.alloc<int>(n_u);
     k_inorder_rep<<<grid_for(n_u), TPB, 0, s>>>(n_u, to.inorder_u, u.urep, inorder_rep);
     check(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s), "D2H");
     st.sync();
     if (herr) raise(herr, "tree build exceeded an internal bound");
-
-    // The node array is final: a second thread copies it to the caller's
-    // host array (pinned staging, DMA on its own stream) while this one
-    // builds the counting layout.
-    struct NodeCopy {
-        kd_node_sink *sink = nullptr;
-        void *host = nullptr;
-        bool handed = false;
-        std::thread th;
-        int code = 0;
-        char msg[160] = "";
-        double ms = 0;
-        ~NodeCopy()
-        {
-            if (th.joinable()) th.join();
-            if (host && !handed) sink->release(host);
-        }
-    } nc;
-    if (sink) {
-        const size_t nbytes = sizeof(NodeRec) * (size_t)memsize;
-        nc.sink = sink;
-        nc.host = sink->alloc(nbytes);
-        if (!nc.host) raise(KD_ENOMEM, "out of host memory for the node array");
-        int dev = 0;
-        check(cudaGetDevice(&dev), "cudaGetDevice");
-        const void *src = to.nodes;
-        NodeCopy *ncp = &nc;
-        auto job = [ncp, dev, src, nbytes] {
-            const double t0 = wall_ms();
-            try {
-                check(cudaSetDevice(dev), "cudaSetDevice");
-                copy_to_pageable(ncp->host, src, nbytes);
-            } catch (const Error &e) {
-                ncp->code = e.code;
-                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %.140s", e.msg);
-            } catch (const std::exception &e) {
-                ncp->code = KD_EINTERNAL;
-                snprintf(ncp->msg, sizeof ncp->msg, "node copy: %s", e.what());
-            }
-            ncp->ms = wall_ms() - t0;
-        };
-        try {
-            nc.th = std::thread(job);
-        } catch (const std::exception &) {
-            job();  // no thread to spare: copy here, before the layout
-        }
-    }
 
     check(cudaEventRecord(ph[4], s), "event");
     // ---- counting layout
@@ -1579,7 +1647,7 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
         check(cudaEventRecord(done[c & 1], st.s), "event");
     };
     const unsigned hw = std::thread::hardware_concurrency();
-    const int nthr = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+    const int nthr = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
     issue(0);
     for (size_t c = 0; c < nch; c++) {
         check(cudaEventSynchronize(done[c & 1]), "D2H wait");

@@ -138,8 +138,10 @@ typedef struct kd_build_stats {
     double ms_levels;     /* device: the level-by-level tree build */
     double ms_layout;     /* device: counting layout, runs, blocks, summaries */
     double ms_device;     /* device: first to last event of the build */
-    double ms_node_copy;  /* host: node array to the returned host array, wall
-                           * (overlapped with the counting layout) */
+    double ms_node_copy;  /* host: node array to the returned host array, wall,
+                           * from the start of the level loop (the copy follows
+                           * the levels as they are built, then overlaps the
+                           * counting layout) */
     double ms_node_wait;  /* host: how long the build then waited for that copy */
     double ms_total_host; /* host: the whole tree_construct call, wall */
     int levels;           /* tree levels built */
