@@ -51,13 +51,7 @@ constexpr int kQ = KD_QPL;              // query points per lane
 constexpr int kTileWarpsPerCta = 4;
 constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
-// 1: in mixed mode, a record is counted together with the next one of its
-// block when both have the same tree field, edge window and histogram and
-// their runs fit 2 * KD_RUN_MAX staged points (one pass, one epilogue)
-#ifndef KD_PAIR_RUNS
-#define KD_PAIR_RUNS 0
-#endif
-constexpr int kStageMax = KD_PAIR_RUNS ? 2 * KD_RUN_MAX : KD_RUN_MAX;  // staged points
+constexpr int kStageMax = KD_RUN_MAX;  // points staged per pass
 constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
 constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
 constexpr int kRunPerLane = KD_RUN_MAX / 32;  // staged run points per lane
@@ -463,22 +457,20 @@ __device__ __forceinline__ void fp64_run(const double *__restrict__ tx,
     }
 }
 
-// Warp-cooperative exact recount of one query over a pass's points (one run
-// [rs, rs + rl), or two when a second run [rsn, rsn + rln) was paired with
-// it): every lane takes the points j = lane, lane + 32, ... (at most
-// 2 * KD_RUN_MAX / 32, so the warp sum of each per-edge count is at most
-// 2 * KD_RUN_MAX <= 128: the four byte-packed counts add without carries in
-// one reduction).  Returns the packed counts in all lanes.
+// Warp-cooperative exact recount of one query over a run: every lane takes
+// the points j = lane, lane + 32, ... (at most KD_RUN_MAX / 32, so the warp
+// sum of each per-edge count is at most KD_RUN_MAX <= 128: the four
+// byte-packed counts add without carries in one reduction).  Returns the
+// packed counts in all lanes.
 __device__ __noinline__ unsigned exact_pass_warp(const double *__restrict__ tx,
                                                  const double *__restrict__ ty,
-                                                 const double *__restrict__ tz, int rs, int rl,
-                                                 int rsn, int rln, double qx, double qy, double qz,
+                                                 const double *__restrict__ tz, int rl,
+                                                 double qx, double qy, double qz,
                                                  const double *R, int kn, int lane)
 {
     unsigned part = 0;
-    for (int j = lane; j < rl + rln; j += 32) {
-        const int t = j < rl ? rs + j : rsn + (j - rl);
-        const double d2 = d2_ref(__ldg(tx + t), __ldg(ty + t), __ldg(tz + t), qx, qy, qz);
+    for (int j = lane; j < rl; j += 32) {
+        const double d2 = d2_ref(__ldg(tx + j), __ldg(ty + j), __ldg(tz + j), qx, qy, qz);
 #pragma unroll
         for (int k = 0; k < 4; k++)
             if (k < kn) part += (unsigned)(d2 < R[k]) << (8 * k);
@@ -486,20 +478,17 @@ __device__ __noinline__ unsigned exact_pass_warp(const double *__restrict__ tx,
     return __reduce_add_sync(0xffffffffu, part);
 }
 
-// Exact recount of one query over a pass's points (global FP64 coordinates,
-// one or two runs as above), for band rechecks and edges FP32 cannot
-// represent; counts packed one per byte.  Out of line so the FP32 loop stays
-// small.
+// Exact recount of one query over a run (global FP64 coordinates), for band
+// rechecks and edges FP32 cannot represent; counts packed one per byte.  Out
+// of line so the FP32 loop stays small.
 __device__ __noinline__ unsigned exact_pass(const double *__restrict__ tx,
                                             const double *__restrict__ ty,
-                                            const double *__restrict__ tz, int rs, int rl, int rsn,
-                                            int rln, double qx, double qy, double qz,
-                                            const double *R, int kn)
+                                            const double *__restrict__ tz, int rl, double qx,
+                                            double qy, double qz, const double *R, int kn)
 {
     int c4[4] = {0, 0, 0, 0};
-    for (int j = 0; j < rl + rln; j++) {
-        const int t = j < rl ? rs + j : rsn + (j - rl);
-        const double d2 = d2_ref(__ldg(tx + t), __ldg(ty + t), __ldg(tz + t), qx, qy, qz);
+    for (int j = 0; j < rl; j++) {
+        const double d2 = d2_ref(__ldg(tx + j), __ldg(ty + j), __ldg(tz + j), qx, qy, qz);
 #pragma unroll
         for (int k = 0; k < 4; k++)
             if (k < kn) c4[k] += d2 < R[k];
@@ -727,9 +716,9 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             }
         };
 
-        // stage the prefetched run at stage offset at (mixed mode); returns
-        // whether its leaf lies in FP32 range of the block centre
-        auto stage_run = [&](int rl_, int at) {
+        // stage the prefetched run (mixed mode); returns whether its leaf
+        // lies in FP32 range of the block centre
+        auto stage_run = [&](int rl_) {
             const double ex = ncx - ox, ey = ncy - oy, ez = ncz - oz;
             const bool in_range = ex * ex + ey * ey + ez * ez < ws->cmax2;
             const float dx = (float)ex, dy = (float)ey, dz = (float)ez;
@@ -743,8 +732,8 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                     const float lz = fmaf(-0.5f, npt[h].z, dz);
                     const float X = -2.0f * lx, Y = -2.0f * ly, Z = -2.0f * lz;
                     const float N = fmaf(lz, lz, fmaf(ly, ly, lx * lx));
-                    ws->stage[2 * (at + j)] = make_float4(X, X, Y, Y);
-                    ws->stage[2 * (at + j) + 1] = make_float4(Z, Z, N, N);
+                    ws->stage[2 * j] = make_float4(X, X, Y, Y);
+                    ws->stage[2 * j + 1] = make_float4(Z, Z, N, N);
                 }
             }
             return in_range;
@@ -755,12 +744,11 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             const uint4 rec = nrec;
             const int rs = (int)rec.x, rl1 = rec.z & 0xFF, tf = (rec.z >> 8) & 0xFF;
             const int k0 = (rec.z >> 16) & 0xFF, K = rec.z >> 24;
-            int rsn = 0, rln = 0;  // a second run counted in the same pass
             // commit the staged run
             bool fp32_range = false;
             if (K != 0) {
                 if (MODE == KD_MODE_MIXED) {
-                    fp32_range = stage_run(rl1, 0);
+                    fp32_range = stage_run(rl1);
                 } else {
                     const int rl = rl1;
                     if (lane < rl) {
@@ -777,24 +765,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
             }
             __syncwarp();
             if (i + 1 < ecnt) issue(i + 1);
-            if (KD_PAIR_RUNS && MODE == KD_MODE_MIXED && K != 0 && fp32_range && i + 1 < ecnt &&
-                (nrec.z >> 8) == (rec.z >> 8) && nrec.w == rec.w &&
-                rl1 + (int)(nrec.z & 0xFF) <= kStageMax) {
-                // same tree field, first edge, edge count and histogram: stage
-                // the next run behind this one when its leaf is in FP32 range
-                // (the centre test is the same on every lane)
-                const int rl_n = nrec.z & 0xFF;
-                const double ex = ncx - ox, ey = ncy - oy, ez = ncz - oz;
-                if (ex * ex + ey * ey + ez * ez < ws->cmax2) {
-                    stage_run(rl_n, rl1);
-                    rsn = (int)nrec.x;
-                    rln = rl_n;
-                    __syncwarp();
-                    i++;
-                    if (i + 1 < ecnt) issue(i + 1);
-                }
-            }
-            const int rl = rl1 + rln;  // staged points of this pass
+            const int rl = rl1;
 
             const int key = tf | (int)(rec.w << 8);
             if (key != cur_tf || since + rl > 0xFFFF) {
@@ -880,7 +851,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                         const int pq = __shfl_sync(0xffffffffu, __ffs(redo) - 1, src);
                         const int qi = qs + kQ * src + pq;
                         const unsigned pk =
-                            exact_pass_warp(J.tx, J.ty, J.tz, rs, rl1, rsn, rln, J.Q.x[qi],
+                            exact_pass_warp(J.tx + rs, J.ty + rs, J.tz + rs, rl, J.Q.x[qi],
                                             J.Q.y[qi], J.Q.z[qi], R + k0 + kb, kn, lane);
                         if (lane == src) {
                             // replace query pq's half-word (selects, no indexing)
@@ -902,7 +873,7 @@ __global__ void __launch_bounds__(32 * kTileWarpsPerCta, 4) k_tiles(TileArgs A)
                 for (int p = 0; p < kQ; p++)
                     if ((redo >> p) & 1) {
                         const unsigned pk =
-                            exact_pass(J.tx, J.ty, J.tz, rs, rl1, rsn, rln, J.Q.x[qbase + p],
+                            exact_pass(J.tx + rs, J.ty + rs, J.tz + rs, rl, J.Q.x[qbase + p],
                                        J.Q.y[qbase + p], J.Q.z[qbase + p], R + k0 + kb, kn);
                         const int sh = 16 * (p & 1);
 #pragma unroll

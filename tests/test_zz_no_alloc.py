@@ -46,24 +46,27 @@ def test_static_scratch_count_matches_allocating_count_on_consecutive_calls():
             N.destroy(t)
 
 
-def _fields_catalog(seed, n, ids, num_fields):
-    """Clustered points whose field ids run over 0 .. ids-1, declared with
-    num_fields fields (the reference's counter is qfield * Fq + tfield, so
-    with Fq != Ft several (qfield, tfield) pairs share one slot)."""
+def _fields_catalog(seed, n, ids, num_fields, axis):
+    """Clustered points whose field ids run over 0 .. ids-1 in slabs along
+    one axis, declared with num_fields fields (the reference's counter is
+    qfield * Fq + tfield, so with Fq != Ft several (qfield, tfield) pairs
+    share one slot)."""
     rs = np.random.RandomState(seed)
     c = rs.rand(n // 100, 3)
     p = (c[rs.randint(0, len(c), n)] + rs.normal(0, 0.01, (n, 3))) % 1.0
-    f = np.minimum((p[:, 1] * ids).astype(np.int32), ids - 1)
+    f = np.minimum((p[:, axis] * ids).astype(np.int32), ids - 1)
     return N.build_tree(np.ascontiguousarray(p), f, num_fields)
 
 
 def test_static_scratch_count_with_unequal_field_counts():
     # query 2 fields / tree 3 fields: slots qf*2 + tf, (0,2) and (1,0) share
     # slot 2; query declared with 3 fields but ids 0..1 against a 2-field tree
-    q2 = _fields_catalog(21, 30_000, 2, 2)
-    t3 = _fields_catalog(22, 50_000, 3, 3)
-    q3 = _fields_catalog(23, 30_000, 2, 3)
-    t2 = _fields_catalog(24, 50_000, 2, 2)
+    # query fields in slabs along x, tree fields along y: every (qfield,
+    # tfield) combination has close pairs
+    q2 = _fields_catalog(21, 30_000, 2, 2, 0)
+    t3 = _fields_catalog(22, 50_000, 3, 3, 1)
+    q3 = _fields_catalog(23, 30_000, 2, 3, 0)
+    t2 = _fields_catalog(24, 50_000, 2, 2, 1)
     radii = np.array([0.002, 0.01, 0.02, 0.05])
     try:
         cases = [(t3, q2), (t2, q3)]
