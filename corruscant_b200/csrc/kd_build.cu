@@ -1136,10 +1136,11 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     check(cudaMemcpyAsync(A[0], iota, sizeof(int) * (size_t)n_u, cudaMemcpyDeviceToDevice, s),
           "copy");
     // superkey 2 = (z, x, y): stable sort of the (x, y, z) order by z
-    sort_pairs(pool, s, u.ukz, ksrt, (const int *)iota, A[2], n_u, 0, 64);
+    // (only the bits that vary among the points: the same order)
+    sort_pairs(pool, s, u.ukz, ksrt, (const int *)iota, A[2], n_u, bit_lo(hv[2]), bit_hi(hv[2]));
     // superkey 1 = (y, z, x): stable sort of the (z, x, y) order by y
     k_gather_u64<<<grid_for(n_u), TPB, 0, s>>>(u.uky, A[2], n_u, ktmp);
-    sort_pairs(pool, s, ktmp, ksrt, (const int *)A[2], A[1], n_u, 0, 64);
+    sort_pairs(pool, s, ktmp, ksrt, (const int *)A[2], A[1], n_u, bit_lo(hv[1]), bit_hi(hv[1]));
 
     check(cudaEventRecord(ph[3], s), "event");
     // ---- tree
