@@ -1025,6 +1025,29 @@ template <class T> static T read1(const T *d, cudaStream_t s)
 
 static void copy_to_pageable(void *dst, const void *src, size_t bytes);
 
+// Touch one byte of every 4 KiB page of [p, p + bytes), split over up to 16
+// threads, so that the pages are resident before they are copied into.
+static void prefault(void *p, size_t bytes)
+{
+    if (bytes < ((size_t)64 << 20)) return;
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthr = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+    auto touch = [p, bytes, nthr](int t) {
+        volatile char *c = (volatile char *)p;
+        const size_t a = bytes * t / nthr, b = bytes * (t + 1) / nthr;
+        for (size_t i = a & ~(size_t)4095; i < b; i += 4096)
+            if (i >= a) c[i] = 0;
+    };
+    std::vector<std::thread> th;
+    try {
+        for (int t = 1; t < nthr; t++) th.emplace_back(touch, t);
+    } catch (const std::exception &) {
+    }
+    touch(0);
+    for (int t = (int)th.size() + 1; t < nthr; t++) touch(t);  // threads not started
+    for (auto &x : th) x.join();
+}
+
 static double wall_ms()
 {
     return std::chrono::duration<double, std::milli>(
@@ -1259,10 +1282,15 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         check(cudaGetDevice(&dev), "cudaGetDevice");
         const char *src = (const char *)to.nodes;
         NodeCopy *ncp = &nc;
-        auto job = [ncp, dev, src] {
+        auto job = [ncp, dev, src, node_bytes] {
             const double t0 = wall_ms();
             try {
                 check(cudaSetDevice(dev), "cudaSetDevice");
+                // fault the whole host array in first, on parallel threads,
+                // while the first levels are built: the copies then write
+                // resident pages instead of taking a page fault (and the
+                // kernel's zeroing of a fresh page) at every page
+                prefault(ncp->host, node_bytes);
                 for (;;) {
                     NodeCopy::Item it;
                     {

@@ -52,11 +52,7 @@ constexpr int kTileWarpsPerCta = 4;
 constexpr int kMaxDistinctQf = 8;       // own fields reduced per warp at a flush
 constexpr int kPass32 = 4;              // edges per FP32 pass (register budget)
 constexpr int kStageMax = KD_RUN_MAX;  // points staged per pass
-// experiment: in mixed mode, this many CTAs per SM run the FP64 tile kernel
-// concurrently on a second stream, pulling blocks from the same queue
-#ifndef KD_HYBRID_FP64_CTAS
-#define KD_HYBRID_FP64_CTAS 0
-#endif
+
 constexpr int kCoopMax = 32;            // rechecks of a run done by the whole warp
 constexpr int kShardChunk = 32;         // blocks per interleaved shard chunk
 constexpr int kRunPerLane = KD_RUN_MAX / 32;  // staged run points per lane
@@ -1171,27 +1167,10 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
         ta.work = work;
         ta.stats = dstats;
         check(cudaMemsetAsync(work, 0, sizeof(int), s), "memset");
-        if (KD_HYBRID_FP64_CTAS > 0 && mode == KD_MODE_MIXED && occ > KD_HYBRID_FP64_CTAS) {
-            const size_t smem64 = tile_smem(ne, KD_MODE_FP64);
-            check(cudaFuncSetAttribute(k_tiles<KD_MODE_FP64>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem64),
-                  "smem attribute");
-            Stream st2;
-            check(cudaEventRecord(ev.e[5], s), "event");
-            check(cudaStreamWaitEvent(st2.s, ev.e[5], 0), "wait");
-            kern<<<nsm * (occ - KD_HYBRID_FP64_CTAS), 32 * kTileWarpsPerCta, smem, s>>>(ta);
-            k_tiles<KD_MODE_FP64><<<nsm * KD_HYBRID_FP64_CTAS, 32 * kTileWarpsPerCta, smem64,
-                                    st2.s>>>(ta);
-            check(cudaEventRecord(ev.e[6], st2.s), "event");
-            check(cudaStreamWaitEvent(s, ev.e[6], 0), "wait");
-            launches += 2;
-        } else {
-            const int grid = (int)std::min<long long>(
-                ((long long)(b1 - b0) + kTileWarpsPerCta - 1) / kTileWarpsPerCta,
-                (long long)nsm * occ);
-            kern<<<grid, 32 * kTileWarpsPerCta, smem, s>>>(ta);
-            launches++;
-        }
+        const int grid = (int)std::min<long long>(
+            ((long long)(b1 - b0) + kTileWarpsPerCta - 1) / kTileWarpsPerCta, (long long)nsm * occ);
+        kern<<<grid, 32 * kTileWarpsPerCta, smem, s>>>(ta);
+        launches++;
         tile_launches++;
         KD_LAUNCH_CHECK("k_tiles");
         check(cudaEventRecord(ev.e[3], s), "event");
