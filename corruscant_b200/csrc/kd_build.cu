@@ -1675,27 +1675,83 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
               "D2H");
         check(cudaEventRecord(done[c & 1], st.s), "event");
     };
-    const unsigned hw = std::thread::hardware_concurrency();
-    const int nthr = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+    // host copies of each chunk fanned out over a pool of threads made once
+    // for the whole call (a chunk takes ~1 ms; creating threads per chunk
+    // would cost a good part of that)
+    struct FanOut {
+        int nthr = 1;
+        std::vector<std::thread> th;
+        std::mutex mu;
+        std::condition_variable go, done;
+        size_t gen = 0;
+        int pending = 0;
+        bool stop = false;
+        char *to = nullptr;
+        const char *from = nullptr;
+        size_t len = 0;
+        void slice(int t, char *d, const char *f, size_t n)
+        {
+            const size_t a = n * t / nthr, b = n * (t + 1) / nthr;
+            std::memcpy(d + a, f + a, b - a);
+        }
+        void worker(int t)
+        {
+            size_t seen = 0;
+            std::unique_lock<std::mutex> g(mu);
+            for (;;) {
+                go.wait(g, [&] { return stop || gen != seen; });
+                if (stop) return;
+                seen = gen;
+                char *d = to;
+                const char *f = from;
+                const size_t n = len;
+                g.unlock();
+                slice(t, d, f, n);
+                g.lock();
+                if (--pending == 0) done.notify_one();
+            }
+        }
+        void copy(char *d, const char *f, size_t n)
+        {
+            {
+                std::lock_guard<std::mutex> g(mu);
+                to = d;
+                from = f;
+                len = n;
+                pending = (int)th.size();
+                gen++;
+            }
+            go.notify_all();
+            // slices of the threads that could not be started are done here
+            for (int t = (int)th.size() + 1; t < nthr; t++) slice(t, d, f, n);
+            slice(0, d, f, n);
+            std::unique_lock<std::mutex> g(mu);
+            done.wait(g, [&] { return pending == 0; });
+        }
+        ~FanOut()
+        {
+            {
+                std::lock_guard<std::mutex> g(mu);
+                stop = true;
+            }
+            go.notify_all();
+            for (auto &x : th) x.join();
+        }
+    } fan;
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        fan.nthr = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+        try {
+            for (int t = 1; t < fan.nthr; t++) fan.th.emplace_back(&FanOut::worker, &fan, t);
+        } catch (const std::exception &) {  // fewer threads: the rest is copied by this one
+        }
+    }
     issue(0);
     for (size_t c = 0; c < nch; c++) {
         check(cudaEventSynchronize(done[c & 1]), "D2H wait");
         if (c + 1 < nch) issue(c + 1);  // into the other buffer, already drained
         const size_t off = c * chunk, len = std::min(chunk, bytes - off);
-        const char *from = (const char *)pin[c & 1];
-        char *to = (char *)dst + off;
-        std::vector<std::thread> th;
-        bool spawned = true;
-        try {
-            for (int t = 1; t < nthr; t++) {
-                const size_t a = len * t / nthr, b = len * (t + 1) / nthr;
-                th.emplace_back([=] { std::memcpy(to + a, from + a, b - a); });
-            }
-        } catch (const std::exception &) {  // no more threads: this one copies the chunk
-            spawned = false;
-        }
-        std::memcpy(to, from, spawned ? len / nthr : len);
-        for (auto &x : th) x.join();
+        fan.copy((char *)dst + off, (const char *)pin[c & 1], len);
     }
 }
 
