@@ -66,7 +66,8 @@ static_assert(sizeof(NodeRec) == 40, "node_t is 40 bytes");
 constexpr int kSmallSeg = 256;
 // Positions per block in the parallel variance kernels (<= kSmallSeg + 1 so a
 // block touches at most two segments).
-constexpr int kVarChunk = 256;
+constexpr int kVarChunk = 256;   // positions per k_var_par block
+constexpr int kVarThreads = 64;  // threads per k_var_par block (4 positions each)
 
 // Once per device (any thread may get here first; doing it twice is harmless):
 // keep freed stream-ordered allocations in the device's pool instead of
@@ -265,82 +266,122 @@ __global__ void k_seg_setup(Segs sg, int ub, LevelBufs lb)
 
 // Parallel sums for big segments: pass 0 accumulates S_j = sum v_j and
 // A_j = sum |v_j|; pass 1 accumulates V_j = sum (v_j - S_j/n)^2.
+// c0, c1, c2: the x of the point at each position of superkey order 0, the
+// y along order 1, the z along order 2 (carried through the partitions), so
+// a segment's coordinates are read contiguously; the parallel sums do not
+// depend on the order within a segment
 template <int PASS>
-__global__ void __launch_bounds__(256) k_var_par(int n_u, const int *__restrict__ pos_seg, Segs sg,
-                                                 LevelBufs lb, const int *__restrict__ args0,
-                                                 const double *__restrict__ ux,
-                                                 const double *__restrict__ uy,
-                                                 const double *__restrict__ uz)
+__global__ void __launch_bounds__(kVarThreads) k_var_par(int n_u, const int *__restrict__ pos_seg,
+                                                         Segs sg, LevelBufs lb,
+                                                         const double *__restrict__ c0,
+                                                         const double *__restrict__ c1,
+                                                         const double *__restrict__ c2)
 {
-    __shared__ double sh[2][6];
-    __shared__ int s_first;
-    if (threadIdx.x < 12) sh[threadIdx.x / 6][threadIdx.x % 6] = 0.0;
-    if (threadIdx.x == 0) s_first = 0x7fffffff;
-    __syncthreads();
-    int base = blockIdx.x * kVarChunk;
+    // pass 0: S0 S1 S2 A0 A1 A2; pass 1: V0 V1 V2
+    constexpr int NV = PASS == 0 ? 6 : 3;
+    constexpr int PER = kVarChunk / kVarThreads;
+    constexpr int NW = kVarThreads / 32;
+    __shared__ double wsum[NW][2][NV];
+    __shared__ double mu_sh[2][3];
+    __shared__ int wmin[NW];
+    const int base = blockIdx.x * kVarChunk;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int seg[PER];
     int smin = 0x7fffffff;
-    for (int k = 0; k < kVarChunk / 256; k++) {
-        int i = base + threadIdx.x + 256 * k;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const int i = base + threadIdx.x + kVarThreads * k;
+        seg[k] = -1;
         if (i < n_u) {
-            int s = pos_seg[i];
-            if (s >= 0 && lb.big[s]) smin = min(smin, s);
+            const int s = pos_seg[i];
+            if (s >= 0 && lb.big[s]) {
+                seg[k] = s;
+                smin = min(smin, s);
+            }
         }
     }
-    atomicMin(&s_first, smin);
+    smin = __reduce_min_sync(0xffffffffu, smin);
+    if (lane == 0) wmin[w] = smin;
     __syncthreads();
-    int s0 = s_first;
+    int s0 = wmin[0];
+#pragma unroll
+    for (int q = 1; q < NW; q++) s0 = min(s0, wmin[q]);
     if (s0 == 0x7fffffff) return;
-    double a[2][6];
+    if (PASS == 1) {  // the means of the chunk's first two segments, once
+        if (threadIdx.x < 6) {
+            const int q = threadIdx.x / 3, j = threadIdx.x % 3, sq = s0 + q;
+            mu_sh[q][j] = sq < *sg.count
+                              ? lb.acc[9 * (size_t)sq + j] / (double)(sg.r[sq] - sg.l[sq] + 1)
+                              : 0.0;
+        }
+        __syncthreads();
+    }
+    double a[2][NV];
 #pragma unroll
     for (int q = 0; q < 2; q++)
 #pragma unroll
-        for (int k = 0; k < 6; k++) a[q][k] = 0.0;
-    for (int k = 0; k < kVarChunk / 256; k++) {
-        int i = base + threadIdx.x + 256 * k;
-        if (i >= n_u) break;
-        int s = pos_seg[i];
-        if (s < 0 || !lb.big[s]) continue;
-        int pt = args0[i];
-        double v[3] = {ux[pt], uy[pt], uz[pt]};
-        double c[6];
+        for (int j = 0; j < NV; j++) a[q][j] = 0.0;
+    bool second = false;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const int s = seg[k];
+        if (s < 0) continue;
+        const int i = base + threadIdx.x + kVarThreads * k;
+        const double v[3] = {c0[i], c1[i], c2[i]};
+        double c[NV];
+        const int slot = s - s0;
         if (PASS == 0) {
+#pragma unroll
             for (int j = 0; j < 3; j++) {
                 c[j] = v[j];
                 c[3 + j] = fabs(v[j]);
             }
         } else {
-            double n = (double)(sg.r[s] - sg.l[s] + 1);
+            const double n = (double)(sg.r[s] - sg.l[s] + 1);
+#pragma unroll
             for (int j = 0; j < 3; j++) {
-                double mu = lb.acc[9 * (size_t)s + j] / n;
-                double d = v[j] - mu;
+                const double mu = slot < 2 ? mu_sh[slot][j] : lb.acc[9 * (size_t)s + j] / n;
+                const double d = v[j] - mu;
                 c[j] = d * d;
-                c[3 + j] = 0.0;
             }
         }
-        int slot = s - s0;
-        if (slot < 2) {
-            for (int j = 0; j < 6; j++) a[slot][j] += c[j];
-        } else {  // not expected (a chunk spans at most two segments)
-            for (int j = 0; j < 6; j++)
-                if (PASS == 0) atomicAdd(&lb.acc[9 * (size_t)s + j], c[j]);
-                else if (j < 3) atomicAdd(&lb.acc[9 * (size_t)s + 6 + j], c[j]);
+        if (slot == 0) {
+#pragma unroll
+            for (int j = 0; j < NV; j++) a[0][j] += c[j];
+        } else if (slot == 1) {
+            second = true;
+#pragma unroll
+            for (int j = 0; j < NV; j++) a[1][j] += c[j];
+        } else {  // a third segment in one chunk: segments this small are rare
+#pragma unroll
+            for (int j = 0; j < NV; j++)
+                atomicAdd(&lb.acc[9 * (size_t)s + (PASS == 0 ? 0 : 6) + j], c[j]);
         }
     }
-    for (int q = 0; q < 2; q++)
-        for (int j = 0; j < 6; j++) {
+    // warp sums; the second segment's only where a lane of the warp holds one
+    const bool two = __any_sync(0xffffffffu, second);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        if (q == 1 && !two) {
+            if (lane < NV) wsum[w][1][lane] = 0.0;
+            break;
+        }
+#pragma unroll
+        for (int j = 0; j < NV; j++) {
             double v = a[q][j];
+#pragma unroll
             for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&sh[q][j], v);
+            if (lane == 0) wsum[w][q][j] = v;
         }
+    }
     __syncthreads();
-    if (threadIdx.x < 12) {
-        int q = threadIdx.x / 6, j = threadIdx.x % 6;
-        int s = s0 + q;
-        if (s < *sg.count && lb.big[s]) {
-            double v = sh[q][j];
-            if (PASS == 0) atomicAdd(&lb.acc[9 * (size_t)s + j], v);
-            else if (j < 3) atomicAdd(&lb.acc[9 * (size_t)s + 6 + j], v);
-        }
+    if (threadIdx.x < 2 * NV) {
+        const int q = threadIdx.x / NV, j = threadIdx.x % NV, s = s0 + q;
+        double v = wsum[0][q][j];
+#pragma unroll
+        for (int x = 1; x < NW; x++) v += wsum[x][q][j];
+        if (v != 0.0 && s < *sg.count && lb.big[s])
+            atomicAdd(&lb.acc[9 * (size_t)s + (PASS == 0 ? 0 : 6) + j], v);
     }
 }
 
@@ -384,10 +425,11 @@ __global__ void k_var_decide(Segs sg, int ub, LevelBufs lb)
 // max_variance_dim exactly as the reference evaluates it (kdbuild.c:308-351),
 // one thread per segment; the three dimensions' chains are independent and
 // are interleaved for latency hiding without changing any chain's order.
-__global__ void k_var_seq(Segs sg, int ub, LevelBufs lb, const int *__restrict__ a0,
-                          const int *__restrict__ a1, const int *__restrict__ a2,
-                          const double *__restrict__ ux, const double *__restrict__ uy,
-                          const double *__restrict__ uz)
+// c0, c1, c2 as for k_var_par: c_j[i] is coordinate j of the point at
+// position i of superkey order j, so the sums below run over exactly the
+// values, in exactly the order, of the reference's loops over args[j]
+__global__ void k_var_seq(Segs sg, int ub, LevelBufs lb, const double *__restrict__ c0,
+                          const double *__restrict__ c1, const double *__restrict__ c2)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= ub || s >= *sg.count) return;
@@ -398,19 +440,12 @@ __global__ void k_var_seq(Segs sg, int ub, LevelBufs lb, const int *__restrict__
     double m0 = 0.0, m1 = 0.0, m2 = 0.0;
     int i = l;
     for (; i + 4 <= r + 1; i += 4) {
-        int p0[4], p1[4], p2[4];
         double v0[4], v1[4], v2[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            p0[k] = a0[i + k];
-            p1[k] = a1[i + k];
-            p2[k] = a2[i + k];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            v0[k] = ux[p0[k]];
-            v1[k] = uy[p1[k]];
-            v2[k] = uz[p2[k]];
+            v0[k] = c0[i + k];
+            v1[k] = c1[i + k];
+            v2[k] = c2[i + k];
         }
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -420,9 +455,9 @@ __global__ void k_var_seq(Segs sg, int ub, LevelBufs lb, const int *__restrict__
         }
     }
     for (; i <= r; i++) {
-        m0 = __dadd_rn(m0, ux[a0[i]]);
-        m1 = __dadd_rn(m1, uy[a1[i]]);
-        m2 = __dadd_rn(m2, uz[a2[i]]);
+        m0 = __dadd_rn(m0, c0[i]);
+        m1 = __dadd_rn(m1, c1[i]);
+        m2 = __dadd_rn(m2, c2[i]);
     }
     double nn = (double)size;
     m0 = __ddiv_rn(m0, nn);
@@ -431,19 +466,12 @@ __global__ void k_var_seq(Segs sg, int ub, LevelBufs lb, const int *__restrict__
     double q0 = 0.0, q1 = 0.0, q2 = 0.0;
     i = l;
     for (; i + 4 <= r + 1; i += 4) {
-        int p0[4], p1[4], p2[4];
         double v0[4], v1[4], v2[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            p0[k] = a0[i + k];
-            p1[k] = a1[i + k];
-            p2[k] = a2[i + k];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            v0[k] = ux[p0[k]];
-            v1[k] = uy[p1[k]];
-            v2[k] = uz[p2[k]];
+            v0[k] = c0[i + k];
+            v1[k] = c1[i + k];
+            v2[k] = c2[i + k];
         }
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -454,8 +482,7 @@ __global__ void k_var_seq(Segs sg, int ub, LevelBufs lb, const int *__restrict__
         }
     }
     for (; i <= r; i++) {
-        double d0 = __dsub_rn(ux[a0[i]], m0), d1 = __dsub_rn(uy[a1[i]], m1),
-               d2 = __dsub_rn(uz[a2[i]], m2);
+        double d0 = __dsub_rn(c0[i], m0), d1 = __dsub_rn(c1[i], m1), d2 = __dsub_rn(c2[i], m2);
         q0 = __fma_rn(d0, d0, q0);
         q1 = __fma_rn(d1, d1, q1);
         q2 = __fma_rn(d2, d2, q2);
@@ -556,9 +583,12 @@ __global__ void k_part_flags(int n_u, const int *__restrict__ pos_seg, Segs sg,
     }
 }
 
+// moves index a[i] and its carried coordinate coord[i] to their
+// stable-partition position in out / coord_out
 __global__ void k_part_scatter(int n_u, const int *__restrict__ pos_seg, Segs sg,
                                const int *__restrict__ a, const unsigned char *__restrict__ side,
-                               const unsigned long long *__restrict__ scan, int *out, int *err)
+                               const unsigned long long *__restrict__ scan, int *out,
+                               const double *__restrict__ coord, double *coord_out, int *err)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_u; i += gridDim.x * blockDim.x) {
         int s = pos_seg[i];
@@ -580,6 +610,7 @@ __global__ void k_part_scatter(int n_u, const int *__restrict__ pos_seg, Segs sg
             }
         }
         out[dst] = pt;
+        coord_out[dst] = coord[i];
     }
 }
 
@@ -1164,6 +1195,17 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     // superkey 1 = (y, z, x): stable sort of the (z, x, y) order by y
     k_gather_u64<<<grid_for(n_u), TPB, 0, s>>>(u.uky, A[2], n_u, ktmp);
     sort_pairs(pool, s, ktmp, ksrt, (const int *)A[2], A[1], n_u, bit_lo(hv[1]), bit_hi(hv[1]));
+    // coordinate d of the point at every position of order d, partitioned
+    // along with the order (the variance passes then read contiguously)
+    double *C[3], *CB[3];
+    {
+        const double *uc[3] = {u.ux, u.uy, u.uz};
+        for (int d = 0; d < 3; d++) {
+            C[d] = pool.alloc<double>(n_u);
+            CB[d] = pool.alloc<double>(n_u);
+            k_gather<double><<<grid_for(n_u), TPB, 0, s>>>(uc[d], A[d], n_u, C[d]);
+        }
+    }
 
     check(cudaEventRecord(ph[3], s), "event");
     // ---- tree
@@ -1329,11 +1371,11 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         long long maxsize = (long long)n_u >> lev;
         if (maxsize > kSmallSeg) {
             unsigned gv = blocks_for(n_u, kVarChunk);
-            k_var_par<0><<<gv, 256, 0, s>>>(n_u, pos[cur], S, lb, A[0], u.ux, u.uy, u.uz);
-            k_var_par<1><<<gv, 256, 0, s>>>(n_u, pos[cur], S, lb, A[0], u.ux, u.uy, u.uz);
+            k_var_par<0><<<gv, kVarThreads, 0, s>>>(n_u, pos[cur], S, lb, C[0], C[1], C[2]);
+            k_var_par<1><<<gv, kVarThreads, 0, s>>>(n_u, pos[cur], S, lb, C[0], C[1], C[2]);
             k_var_decide<<<gs, TPB, 0, s>>>(S, ub, lb);
         }
-        k_var_seq<<<blocks_for(ub, 64), 64, 0, s>>>(S, ub, lb, A[0], A[1], A[2], u.ux, u.uy, u.uz);
+        k_var_seq<<<blocks_for(ub, 64), 64, 0, s>>>(S, ub, lb, C[0], C[1], C[2]);
         k_level_nodes<<<gs, TPB, 0, s>>>(S, ub, lb, A[0], A[1], A[2], u, to, err);
         KD_LAUNCH_CHECK("level kernels");
         if (maxsize < 4) break;  // every segment of this level was a base case
@@ -1347,8 +1389,10 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         for (int d = 0; d < 3; d++) {
             k_part_flags<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, A[d], side, pf);
             excl_sum(pool, s, pf, ps, n_u);
-            k_part_scatter<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, A[d], side, ps, B[d], err);
+            k_part_scatter<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, A[d], side, ps, B[d],
+                                                          C[d], CB[d], err);
             std::swap(A[d], B[d]);
+            std::swap(C[d], CB[d]);
         }
         excl_sum(pool, s, lb.haskids, lb.rank, ub);
         k_children<<<gs, TPB, 0, s>>>(S, ub, lb, N, cap, err);
