@@ -89,6 +89,10 @@ def kdlib():
         L = loadlib("libkdtree")
         L.tree_construct.restype = KdTree
         L.tree_construct.argtypes = [POINTER(c_double), POINTER(c_int), c_int, c_int]
+        L.kd_tree_construct_deferred.restype = KdTree
+        L.kd_tree_construct_deferred.argtypes = [POINTER(c_double), POINTER(c_int), c_int, c_int]
+        L.kd_tree_wait_nodes.restype = c_int
+        L.kd_tree_wait_nodes.argtypes = [KdTree]
         L.pair_count.restype = POINTER(c_longlong)
         L.pair_count.argtypes = [KdTree, POINTER(c_double), POINTER(c_int), c_int, c_int,
                                  c_double, c_int]
@@ -154,17 +158,29 @@ def iptr(a):
     return None if a is None else a.ctypes.data_as(POINTER(c_int))
 
 
-def build_tree(points, fields, num_fields):
-    """tree_construct on C-contiguous float64 (N,3) points and int32 fields."""
-    t = kdlib().tree_construct(dptr(points), iptr(fields), c_int(points.shape[0]),
-                               c_int(num_fields))
+def build_tree(points, fields, num_fields, deferred=False):
+    """tree_construct on C-contiguous float64 (N,3) points and int32 fields.
+
+    deferred: kd_tree_construct_deferred, which returns once the tree is on
+    the device while its node array is still being copied to node_data; the
+    tree can be counted at once, and wait_nodes(t) waits for the node array.
+    """
+    fn = kdlib().kd_tree_construct_deferred if deferred else kdlib().tree_construct
+    t = fn(dptr(points), iptr(fields), c_int(points.shape[0]), c_int(num_fields))
     if not t.node_data:
         raise_last("tree_construct failed")
     return t
 
 
+def wait_nodes(t):
+    """kd_tree_wait_nodes: returns once t.node_data is complete."""
+    if kdlib().kd_tree_wait_nodes(t) != 0:
+        raise_last()
+
+
 def node_fields(t):
     """Semantic node fields of a kdtree_t as numpy arrays (length memsize)."""
+    wait_nodes(t)
     m = t.memsize
     raw = np.ctypeslib.as_array(ctypes.cast(t.node_data, POINTER(ctypes.c_uint8)),
                                 shape=(m * 40,)).reshape(m, 40)

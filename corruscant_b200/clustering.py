@@ -151,7 +151,7 @@ class tree:
             self.field_sizes = self._calc_field_sizes()
         self.points = np.require(points, dtype="float64", requirements="AC")
         self._make_tree()
-        self.size = self.ctree.size
+        self.size = self._ct.size
         if fields is None:
             self.field_sizes = np.array(self.size)
 
@@ -160,22 +160,40 @@ class tree:
         return np.bincount(self.fields, minlength=self.N_fields)
 
     def _make_tree(self):
-        """Build the GPU tree of ``points`` / ``fields`` into ``ctree``
-        (clustering.py:340-349)."""
-        self.ctree = _native.build_tree(self.points, self.fields, self.N_fields)
+        """Build the GPU tree of ``points`` / ``fields`` (clustering.py:340-349).
+
+        The build returns once the tree is on the device; its node array
+        still drains to the host behind it, so counts can start at once.
+        ``ctree`` waits for the node array before handing out the struct.
+        """
+        self._ct = _native.build_tree(self.points, self.fields, self.N_fields, deferred=True)
+        self._nodes_ready = False
+
+    @property
+    def ctree(self):
+        """The reference's ``kdtree_t``, its ``node_data`` complete."""
+        if self._ct is not None and not self._nodes_ready:
+            _native.wait_nodes(self._ct)
+            self._nodes_ready = True
+        return self._ct
+
+    @ctree.setter
+    def ctree(self, value):
+        self._ct = value
+        self._nodes_ready = True
 
     def __del__(self):
-        ct = getattr(self, "ctree", None)
+        ct = getattr(self, "_ct", None)
         if ct is not None and ct.node_data:
             _native.destroy(ct)
-            self.ctree = None
+            self._ct = None
 
 
 def _query_tree(tree_, points, radius, num_threads, fields=None, N_fields=1):
     """One radius through the reference entry point ``pair_count``
     (clustering.py:73-90): an (N_fields, tree.N_fields) int64 matrix."""
     del num_threads  # the GPU path has no thread count
-    counts = _native.pair_count(tree_.ctree, points, fields, N_fields, radius)
+    counts = _native.pair_count(tree_._ct, points, fields, N_fields, radius)
     return counts.reshape(N_fields, tree_.N_fields)
 
 
@@ -188,7 +206,7 @@ def _count_binned(tree_, query, radii, mode):
 def _count_binned_batch(jobs, radii, mode):
     """_count_binned for several (tree, query) pairs, counted together in one
     device batch (``kd_count_batch``)."""
-    cums = _native.count_batch([(t.ctree, q.ctree) for t, q in jobs], radii, mode=mode)
+    cums = _native.count_batch([(t._ct, q._ct) for t, q in jobs], radii, mode=mode)
     return [np.diff(c.reshape(len(radii), q.N_fields, t.N_fields), axis=0)
             for (t, q), c in zip(jobs, cums)]
 

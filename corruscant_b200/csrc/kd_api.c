@@ -105,7 +105,8 @@ static void *alloc_nodes(size_t nb)
 
 static void release_nodes(void *p) { free(p); }
 
-kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
+static kdtree_t construct(double *xyz, int *fields, int length, int num_fields, int deferred,
+                          const char *who)
 {
     kdtree_t t;
     kd_handle *h;
@@ -114,16 +115,16 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
     memset(&t, 0, sizeof t);
     clear_error();
     if (!xyz || length < 1) {
-        kd_set_error(KD_EINVAL, "tree_construct: need at least one point");
+        kd_set_error(KD_EINVAL, "%s: need at least one point", who);
         return t;
     }
     if (length > KD_MAX_POINTS) {
-        kd_set_error(KD_EINVAL, "tree_construct: %d points, at most %d", length, KD_MAX_POINTS);
+        kd_set_error(KD_EINVAL, "%s: %d points, at most %d", who, length, KD_MAX_POINTS);
         return t;
     }
     h = (kd_handle *)calloc(1, sizeof *h);
     if (!h) {
-        kd_set_error(KD_ENOMEM, "tree_construct: out of host memory");
+        kd_set_error(KD_ENOMEM, "%s: out of host memory", who);
         return t;
     }
     /* every byte of the node array is written by the build's copy: empty
@@ -132,7 +133,7 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
     sink.alloc = alloc_nodes;
     sink.release = release_nodes;
     sink.nodes = NULL;
-    if (kdg_build_tree(xyz, fields, length, num_fields, &sink, &h->cat) != KD_OK) {
+    if (kdg_build_tree(xyz, fields, length, num_fields, &sink, deferred, &h->cat) != KD_OK) {
         free(h);
         return t;
     }
@@ -147,6 +148,25 @@ kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
     t.memsize = h->cat.memsize;
     t.num_fields = num_fields;
     return t;
+}
+
+kdtree_t tree_construct(double *xyz, int *fields, int length, int num_fields)
+{
+    return construct(xyz, fields, length, num_fields, 0, "tree_construct");
+}
+
+kdtree_t kd_tree_construct_deferred(double *xyz, int *fields, int length, int num_fields)
+{
+    return construct(xyz, fields, length, num_fields, 1, "kd_tree_construct_deferred");
+}
+
+int kd_tree_wait_nodes(kdtree_t t)
+{
+    kd_handle *h;
+    clear_error();
+    h = lookup_or_fail(&t, "kd_tree_wait_nodes");
+    if (!h) return KD_EINVAL;
+    return kdg_wait_nodes(&h->cat);
 }
 
 void destroy(kdtree_t t)

@@ -39,6 +39,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <exception>
+#include <memory>
 #include <new>
 #include <cmath>
 #include <cstring>
@@ -86,6 +87,43 @@ void init_device()
     }
     cudaGetLastError();
     done.fetch_or(bit);
+}
+
+// The device pool of the node arrays that builds copy to the host.  It is
+// kept apart from the default pool that every other build and count array
+// comes from: a node array still being copied while a count runs (deferred
+// builds) would otherwise sit inside a cached block of the default pool that
+// the count's large tile-record buffer could have reused, and the pool would
+// grow (new physical memory) for that buffer instead.
+static cudaMemPool_t node_pool()
+{
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    cudaMemPool_t def = nullptr;
+    if (dev < 0 || dev >= 64) {
+        check(cudaDeviceGetDefaultMemPool(&def, dev), "cudaDeviceGetDefaultMemPool");
+        return def;
+    }
+    std::lock_guard<std::mutex> g(mu);
+    if (!pools[dev]) {
+        cudaMemPoolProps props;
+        memset(&props, 0, sizeof props);
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();  // no pool of its own: the default one serves
+            check(cudaDeviceGetDefaultMemPool(&def, dev), "cudaDeviceGetDefaultMemPool");
+            return def;
+        }
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr);
+        pools[dev] = p;
+    }
+    return pools[dev];
 }
 
 // Order-preserving 64-bit key of a double; -0.0 maps to +0.0's key so that
@@ -1085,8 +1123,55 @@ static double wall_ms()
                std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// The node array's way to the caller's host array (see build_impl): the
+// per-level items the build queues, the copier thread that drains them, and,
+// for a deferred build, the device node array it reads until it is done.
+struct NodeCopy {
+    kd_node_sink *sink = nullptr;
+    void *host = nullptr;
+    bool handed = false;
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv;
+    struct Item {
+        cudaEvent_t ev;
+        size_t off, len;
+    };
+    std::vector<Item> items;
+    size_t next = 0;     // first item the copier has not taken
+    bool closed = false; // no more items
+    std::vector<cudaEvent_t> events;
+    int code = 0;
+    char msg[160] = "";
+    double ms = 0;
+    // deferred builds: the device node array (freed once the copy is done)
+    // and the one-time join
+    void *dnodes = nullptr;
+    std::once_flag joined;
+    void push(cudaEvent_t ev, size_t off, size_t len)
+    {
+        std::lock_guard<std::mutex> g(mu);
+        items.push_back({ev, off, len});
+        cv.notify_one();
+    }
+    void close()
+    {
+        std::lock_guard<std::mutex> g(mu);
+        closed = true;
+        cv.notify_one();
+    }
+    ~NodeCopy()
+    {
+        close();
+        if (th.joinable()) th.join();
+        for (auto e : events) cudaEventDestroy(e);
+        if (dnodes) cudaFree(dnodes);
+        if (host && !handed) sink->release(host);
+    }
+};
+
 static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                       int query_only, kd_node_sink *sink, kd_catalog *cat)
+                       int query_only, kd_node_sink *sink, int deferred, kd_catalog *cat)
 {
     init_device();
     Stream st;
@@ -1220,7 +1305,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     }
     TreeOut to;
     to.memsize = memsize;
-    to.nodes = keep.alloc<NodeRec>(memsize);
+    to.nodes = sink ? keep.alloc_from<NodeRec>(node_pool(), memsize) : keep.alloc<NodeRec>(memsize);
     to.npoint = pool.alloc<int>(memsize);
     to.ndim = pool.alloc<unsigned char>(memsize);
     to.inorder_u = pool.alloc<int>(n_u);
@@ -1265,44 +1350,8 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     // level's slots; a second host thread waits for each event and copies
     // the slots (pinned staging, DMA on its own stream) while the build
     // goes on, then the rest once the loop ends, during the counting layout.
-    struct NodeCopy {
-        kd_node_sink *sink = nullptr;
-        void *host = nullptr;
-        bool handed = false;
-        std::thread th;
-        std::mutex mu;
-        std::condition_variable cv;
-        struct Item {
-            cudaEvent_t ev;
-            size_t off, len;
-        };
-        std::vector<Item> items;
-        size_t next = 0;     // first item the copier has not taken
-        bool closed = false; // no more items
-        std::vector<cudaEvent_t> events;
-        int code = 0;
-        char msg[160] = "";
-        double ms = 0;
-        void push(cudaEvent_t ev, size_t off, size_t len)
-        {
-            std::lock_guard<std::mutex> g(mu);
-            items.push_back({ev, off, len});
-            cv.notify_one();
-        }
-        void close()
-        {
-            std::lock_guard<std::mutex> g(mu);
-            closed = true;
-            cv.notify_one();
-        }
-        ~NodeCopy()
-        {
-            close();
-            if (th.joinable()) th.join();
-            for (auto e : events) cudaEventDestroy(e);
-            if (host && !handed) sink->release(host);
-        }
-    } nc;
+    std::unique_ptr<NodeCopy> ncu(new NodeCopy);
+    NodeCopy &nc = *ncu;
     const size_t node_bytes = sizeof(NodeRec) * (size_t)memsize;
     size_t node_queued = sizeof(NodeRec);  // slot 0 is never written: it stays zero
     // queue the node slots [node_queued, upto) once the stream reaches here
@@ -1546,14 +1595,16 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     KD_LAUNCH_CHECK("summary kernels");
     check(cudaEventRecord(ph[5], s), "event");
     st.sync();
-    const double wait0 = wall_ms();
-    if (nc.th.joinable()) nc.th.join();
-    const double waited = wall_ms() - wait0;
-    if (nc.code) raise(nc.code, nc.msg);
     kd_build_stats bs;
     memset(&bs, 0, sizeof bs);
-    bs.ms_node_copy = nc.ms;
-    bs.ms_node_wait = waited;
+    if (!deferred || !sink) {
+        const double wait0 = wall_ms();
+        if (nc.th.joinable()) nc.th.join();
+        const double waited = wall_ms() - wait0;
+        if (nc.code) raise(nc.code, nc.msg);
+        bs.ms_node_copy = nc.ms;
+        bs.ms_node_wait = waited;
+    }
     {
         float ms[5] = {0, 0, 0, 0, 0}, tot = 0;
         for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ph[i], ph[i + 1]);
@@ -1581,9 +1632,11 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     cat->fields_split = split;
     cat->max_abs = maxabs;
     if (sink) {
-        // the host holds the node array; the device copy is freed with the pool
+        // the host holds the node array; the device copy is freed with the
+        // pool, or, while a deferred copy still reads it, once that is done
         sink->nodes = nc.host;
         nc.handed = true;
+        nc.sink = nullptr;
         cat->d_nodes = nullptr;
     } else {
         cat->d_nodes = keep.keep(to.nodes);
@@ -1617,19 +1670,23 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     cat->d_blk_box = keep.keep(bbox);
     cat->device_bytes = keep.bytes;
     cat->bstats = bs;
+    if (sink && deferred) {
+        nc.dnodes = keep.keep(to.nodes);
+        cat->pending = ncu.release();
+    }
 }
 
 }  // namespace kd
 
 static int build_entry(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                       int query_only, kd_node_sink *sink, kd_catalog *cat)
+                       int query_only, kd_node_sink *sink, int deferred, kd_catalog *cat)
 {
     if (n < 1) {
         kd_set_error(KD_EINVAL, "a tree needs at least one point");
         return KD_EINVAL;
     }
     try {
-        kd::build_impl(h_xyz, h_fields, n, num_fields, query_only, sink, cat);
+        kd::build_impl(h_xyz, h_fields, n, num_fields, query_only, sink, deferred, cat);
         return KD_OK;
     } catch (const kd::Error &e) {
         kd_set_error(e.code, "%s", e.msg);
@@ -1646,18 +1703,18 @@ static int build_entry(const double *h_xyz, const int *h_fields, int n, int num_
 extern "C" int kdg_build(const double *h_xyz, const int *h_fields, int n, int num_fields,
                          int query_only, kd_catalog *cat)
 {
-    return build_entry(h_xyz, h_fields, n, num_fields, query_only, nullptr, cat);
+    return build_entry(h_xyz, h_fields, n, num_fields, query_only, nullptr, 0, cat);
 }
 
 extern "C" int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                              kd_node_sink *sink, kd_catalog *cat)
+                              kd_node_sink *sink, int deferred, kd_catalog *cat)
 {
     if (!sink || !sink->alloc || !sink->release) {
         kd_set_error(KD_EINVAL, "kdg_build_tree: no node array sink");
         return KD_EINVAL;
     }
     sink->nodes = nullptr;
-    return build_entry(h_xyz, h_fields, n, num_fields, 0, sink, cat);
+    return build_entry(h_xyz, h_fields, n, num_fields, 0, sink, deferred, cat);
 }
 
 // Runs a catalog operation on the catalog's device, then restores the
@@ -1674,32 +1731,57 @@ struct OnDevice {
 
 namespace kd {
 
-// Device -> pageable host copy of a large array (the node array returned by
-// tree_construct, 1.3 GB at 20M points).  A plain cudaMemcpy into freshly
-// allocated pageable memory runs at the speed of the page faults of its one
-// copying thread; here the data goes through two pinned staging chunks (the
-// next chunk's DMA overlaps the current one's host copy) and each chunk is
-// copied into the destination by several threads, which take the destination's
-// first-touch page faults in parallel.
+// Device -> pageable host copy of the node array returned by tree_construct
+// (1.3 GB at 20M points), one queued item at a time.  A plain cudaMemcpy into
+// pageable memory goes through the driver's own staging, one copy at a time
+// for the whole process, and at the speed of the page faults of its one
+// copying thread; it also makes every other pageable transfer of the process
+// (the build's own small reads of device scalars) queue behind it.  Here the
+// data goes through two pinned staging chunks (the next chunk's DMA overlaps
+// the current one's host copy) and each chunk is copied into the destination
+// by several threads, which take the destination's first-touch page faults in
+// parallel.
+namespace {
+struct Staging {
+    static constexpr size_t kChunk = size_t(32) << 20;
+    void *pin[2] = {nullptr, nullptr};
+};
+// pinned staging pairs kept for the life of the process (allocating pinned
+// memory per copy costs more than the copy): one per copy running at once
+std::mutex g_stage_mu;
+std::vector<Staging *> g_stage_free;
+struct StagingLease {
+    Staging *st = nullptr;
+    StagingLease()
+    {
+        {
+            std::lock_guard<std::mutex> g(g_stage_mu);
+            if (!g_stage_free.empty()) {
+                st = g_stage_free.back();
+                g_stage_free.pop_back();
+                return;
+            }
+        }
+        std::unique_ptr<Staging> n(new Staging);
+        for (int i = 0; i < 2; i++)
+            check(cudaHostAlloc(&n->pin[i], Staging::kChunk, cudaHostAllocPortable),
+                  "cudaHostAlloc");
+        st = n.release();
+    }
+    ~StagingLease()
+    {
+        std::lock_guard<std::mutex> g(g_stage_mu);
+        g_stage_free.push_back(st);
+    }
+};
+}  // namespace
+
 static void copy_to_pageable(void *dst, const void *src, size_t bytes)
 {
-    const size_t chunk = size_t(32) << 20;
-    if (bytes <= chunk) {
-        check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "D2H");
-        return;
-    }
-    // two pinned staging chunks kept for the life of the process (allocating
-    // pinned memory per call costs more than the copy); calls that find them
-    // in use by another thread fall back to a plain copy
-    static std::mutex mu;
-    static void *pin[2] = {nullptr, nullptr};
-    std::unique_lock<std::mutex> lock(mu, std::try_to_lock);
-    if (!lock.owns_lock()) {
-        check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "D2H");
-        return;
-    }
-    for (int i = 0; i < 2; i++)
-        if (!pin[i]) check(cudaHostAlloc(&pin[i], chunk, cudaHostAllocPortable), "cudaHostAlloc");
+    const size_t chunk = Staging::kChunk;
+    if (bytes == 0) return;
+    StagingLease lease;
+    void *const *pin = lease.st->pin;
     Stream st;
     cudaEvent_t done[2] = {nullptr, nullptr};
     struct Release {
@@ -1783,8 +1865,9 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
         }
     } fan;
     {
+        // small items (the top levels) are copied by this thread alone
         const unsigned hw = std::thread::hardware_concurrency();
-        fan.nthr = (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+        fan.nthr = bytes < (size_t(4) << 20) ? 1 : (int)std::max(1u, std::min(16u, hw ? hw : 1u));
         try {
             for (int t = 1; t < fan.nthr; t++) fan.th.emplace_back(&FanOut::worker, &fan, t);
         } catch (const std::exception &) {  // fewer threads: the rest is copied by this one
@@ -1813,8 +1896,36 @@ extern "C" int kdg_copy_inorder(const kd_catalog *cat, int *h_perm)
     return KD_OK;
 }
 
+extern "C" int kdg_wait_nodes(kd_catalog *cat)
+{
+    kd::NodeCopy *nc = (kd::NodeCopy *)cat->pending;
+    if (!nc) return KD_OK;
+    std::call_once(nc->joined, [nc, cat] {
+        const double w0 = kd::wall_ms();
+        if (nc->th.joinable()) nc->th.join();
+        cat->bstats.ms_node_wait = kd::wall_ms() - w0;
+        cat->bstats.ms_node_copy = nc->ms;
+        OnDevice on(cat->device);
+        // the copier has finished reading it: a stream-ordered free, so that
+        // a count still running on the device is not waited for
+        if (nc->dnodes) cudaFreeAsync(nc->dnodes, cudaStreamPerThread);
+        nc->dnodes = nullptr;
+    });
+    if (nc->code) {
+        kd_set_error(nc->code, "%s", nc->msg);
+        return nc->code;
+    }
+    return KD_OK;
+}
+
 extern "C" void kdg_free(kd_catalog *cat)
 {
+    if (cat->pending) {
+        kdg_wait_nodes(cat);
+        OnDevice on(cat->device);
+        delete (kd::NodeCopy *)cat->pending;
+        cat->pending = nullptr;
+    }
     OnDevice on(cat->device);
     void *ptrs[] = {cat->d_nodes,    cat->d_inorder_rep, cat->d_x,       cat->d_y,
                     cat->d_z,        cat->d_qf,          cat->fields_split ? cat->d_tf : nullptr,

@@ -52,6 +52,20 @@ struct Pool {
         bytes += b;
         return (T *)p;
     }
+    // n elements from a given memory pool (stream-ordered like alloc)
+    template <class T> T *alloc_from(cudaMemPool_t mp, size_t n)
+    {
+        void *p = nullptr;
+        size_t b = (n ? n : 1) * sizeof(T);
+        cudaError_t e = cudaMallocFromPoolAsync(&p, b, mp, s);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            raise(KD_ENOMEM, "device allocation failed", e);
+        }
+        ptrs.push_back(p);
+        bytes += b;
+        return (T *)p;
+    }
     // hand ownership of p to the caller (it will not be freed by ~Pool)
     template <class T> T *keep(T *p)
     {

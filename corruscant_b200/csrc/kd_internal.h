@@ -87,6 +87,7 @@ typedef struct kd_catalog {
 
     size_t device_bytes;
     kd_build_stats bstats; /* phase timings of the build */
+    void *pending;         /* deferred builds: the node copy still running */
 } kd_catalog;
 
 /* Build a catalog from host arrays (xyz interleaved (n,3), fields may be
@@ -106,10 +107,15 @@ typedef struct kd_node_sink {
 } kd_node_sink;
 
 /* kdg_build for a tree: the node array (memsize * 40 bytes) is copied into
- * sink's host array while the counting layout is built (the device keeps no
- * copy of it). */
+ * sink's host array while the tree and the counting layout are built (the
+ * device keeps no copy of it).  deferred = 0: returns once the host array is
+ * complete.  deferred = 1: returns once the catalog is complete on the
+ * device (it may be counted at once) while a host thread still fills the
+ * host array; kdg_wait_nodes waits for that thread (KD_OK or the copy's
+ * error, with the message set), and kdg_free waits for it first. */
 int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                   kd_node_sink *sink, kd_catalog *cat);
+                   kd_node_sink *sink, int deferred, kd_catalog *cat);
+int kdg_wait_nodes(kd_catalog *cat);
 /* Copy the in-order permutation (input index of each in-order node). */
 int kdg_copy_inorder(const kd_catalog *cat, int *h_perm);
 void kdg_free(kd_catalog *cat);

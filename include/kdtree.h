@@ -148,8 +148,27 @@ typedef struct kd_build_stats {
     int n_unique;         /* unique points */
 } kd_build_stats;
 
-/* Timing of the build that made `tree`.  Returns 0 or KD_EINVAL. */
+/* Timing of the build that made `tree`.  Returns 0 or KD_EINVAL.  For a
+ * deferred build (kd_tree_construct_deferred) ms_node_copy and ms_node_wait
+ * are filled in by kd_tree_wait_nodes (0 until then) and ms_total_host is the
+ * time until the construct call returned. */
 int kd_tree_build_stats(kdtree_t tree, kd_build_stats *stats);
+
+/* tree_construct (src/kdbuild.c:451-537) that returns before its node array
+ * is complete: once the tree is built on the device, while a host thread is
+ * still copying the node array into node_data.  The tree may be counted at
+ * once (every kd_count_* entry point and pair_count read only the device
+ * copy), which lets the count run while the 40-byte-per-slot node array
+ * (1.3 GB at 20M points) drains to the host.  node_data must not be read
+ * before kd_tree_wait_nodes has returned 0.  destroy waits for the copy
+ * itself.  Errors of the build are returned as tree_construct returns them;
+ * an error of the copy is returned by kd_tree_wait_nodes. */
+kdtree_t kd_tree_construct_deferred(double *xyz, int *fields, int length, int num_fields);
+
+/* Waits until the node array of `tree` is complete.  Returns 0 (at once for
+ * a tree from tree_construct, or one already waited for), the copy's error
+ * code with kd_last_error set, or KD_EINVAL for a tree that is not live. */
+int kd_tree_wait_nodes(kdtree_t tree);
 
 /* Last error of the calling thread: returns its code (0 = none) and copies
  * the message into buf (may be NULL). */

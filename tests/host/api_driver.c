@@ -286,6 +286,34 @@ static void scenario_faults(void)
     t = tree_construct(a.xyz, a.f, a.n, a.nf);
     CHECK(!t.node_data && kd_last_error(NULL, 0) == -6, "copy failure");
     fake_fail_copy = 0;
+    /* deferred builds: counted before the wait; a copy failure is reported
+     * by the wait, and destroy without a wait releases everything */
+    {
+        kdtree_t d = kd_tree_construct_deferred(a.xyz, a.f, a.n, a.nf);
+        long long *want = (long long *)malloc(sizeof(long long) * NR * a.nf * a.nf);
+        CHECK(d.node_data && want, "deferred build");
+        t = tree_construct(a.xyz, a.f, a.n, a.nf);
+        CHECK(kd_count_radii(t, t, RADII, NR, 0, want, NULL) == KD_OK &&
+                  kd_count_radii(d, d, RADII, NR, 0, out, NULL) == KD_OK &&
+                  !memcmp(want, out, sizeof(long long) * NR * a.nf * a.nf),
+              "deferred tree counts");
+        CHECK(kd_tree_wait_nodes(d) == KD_OK && kd_tree_wait_nodes(d) == KD_OK &&
+                  kd_tree_wait_nodes(t) == KD_OK, "waits");
+        destroy(d);
+        CHECK(kd_tree_wait_nodes(d) == KD_EINVAL, "wait on a destroyed tree");
+        destroy(t);
+        free(want);
+        fake_fail_copy = -6;
+        d = kd_tree_construct_deferred(a.xyz, a.f, a.n, a.nf);
+        CHECK(d.node_data && kd_tree_wait_nodes(d) == -6 &&
+                  kd_last_error(msg, sizeof msg) == -6 && strstr(msg, "injected"),
+              "deferred copy failure: %s", msg);
+        destroy(d);
+        d = kd_tree_construct_deferred(a.xyz, a.f, a.n, a.nf);
+        CHECK(d.node_data, "deferred build");
+        destroy(d); /* never waited for */
+        fake_fail_copy = 0;
+    }
     t = tree_construct(a.xyz, a.f, a.n, a.nf);
     fake_fail_count = -8;
     CHECK(kd_count_radii(t, t, RADII, NR, 0, out, NULL) == -8, "count failure");

@@ -20,7 +20,8 @@
 /* ---- failure injection (set by the test driver) */
 int fake_fail_build = 0;  /* error code kdg_build returns, 0 = none */
 int fake_fail_count = 0;  /* error code kdg_count_batch / kdg_count_static return */
-int fake_fail_copy = 0;   /* error code kdg_copy_nodes returns */
+int fake_fail_copy = 0;   /* error code of the node array copy (kdg_build_tree, or
+                           * kdg_wait_nodes for a deferred build) */
 
 typedef struct {
     double *xyz; /* n x 3 */
@@ -79,7 +80,7 @@ oom:
 }
 
 int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fields,
-                   kd_node_sink *sink, kd_catalog *cat)
+                   kd_node_sink *sink, int deferred, kd_catalog *cat)
 {
     int rc;
     void *host;
@@ -87,7 +88,7 @@ int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fiel
     rc = kdg_build(h_xyz, h_fields, n, num_fields, 0, cat);
     if (rc != KD_OK) return rc;
     host = sink->alloc(sizeof(node_t) * (size_t)cat->memsize);
-    if (!host || fake_fail_copy) {
+    if (!host || (fake_fail_copy && !deferred)) {
         if (host) sink->release(host);
         kdg_free(cat);
         rc = host ? fake_fail_copy : KD_ENOMEM;
@@ -98,7 +99,27 @@ int kdg_build_tree(const double *h_xyz, const int *h_fields, int n, int num_fiel
     free(cat->d_nodes);
     cat->d_nodes = NULL;
     sink->nodes = host;
+    if (deferred) {
+        /* the copy "still running": its outcome is reported by the wait */
+        int *code = (int *)malloc(sizeof(int));
+        if (!code) {
+            sink->nodes = NULL;
+            sink->release(host);
+            kdg_free(cat);
+            kd_set_error(KD_ENOMEM, "out of host memory");
+            return KD_ENOMEM;
+        }
+        *code = fake_fail_copy;
+        cat->pending = code;
+    }
     return KD_OK;
+}
+
+int kdg_wait_nodes(kd_catalog *cat)
+{
+    int code = cat->pending ? *(int *)cat->pending : 0;
+    if (code) kd_set_error(code, "injected node copy failure");
+    return code;
 }
 
 int kdg_copy_inorder(const kd_catalog *cat, int *h_perm)
@@ -111,6 +132,7 @@ int kdg_copy_inorder(const kd_catalog *cat, int *h_perm)
 void kdg_free(kd_catalog *cat)
 {
     fake_pts *fp = (fake_pts *)cat->d_x;
+    free(cat->pending);
     if (fp) {
         free(fp->xyz);
         free(fp->f);

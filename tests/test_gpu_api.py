@@ -97,3 +97,40 @@ def test_build_statistics_and_overlapped_node_copy():
             assert np.array_equal(nodes[k], onodes[k]), k
     finally:
         _native.destroy(t)
+
+
+def test_deferred_build_counts_while_node_array_drains():
+    """kd_tree_construct_deferred: the tree counts at once, its node array
+    equals the oracle's after kd_tree_wait_nodes, the copy's timing is filled
+    in by the wait, and a tree never waited for is destroyed cleanly."""
+    rs = np.random.RandomState(9)
+    p = rs.rand(3_000_000, 3)  # a 160 MB node array: several copy items
+    f = (p[:, 1] * 4).astype(np.int32)
+    q = rs.rand(20_000, 3)
+    qf = (q[:, 1] * 4).astype(np.int32)
+    radii = np.array([0.001, 0.004, 0.01])
+    t = _native.build_tree(p, f, 4, deferred=True)
+    tq = _native.build_tree(q, qf, 4, deferred=True)
+    t2 = _native.build_tree(p, f, 4, deferred=True)
+    try:
+        got = _native.count_radii(t, tq, radii)
+        _native.wait_nodes(t)
+        _native.wait_nodes(t)  # a second wait returns at once
+        st = _native.build_stats(t)
+        assert st["ms_node_copy"] > 0 and st["ms_node_wait"] >= 0
+        ot = O.OracleTree(p, f, 4)
+        assert np.array_equal(got, ot.tree_counts(q, qf, 4, radii))
+        nodes, onodes = _native.node_fields(t), ot.nodes()
+        for k in nodes:
+            assert np.array_equal(nodes[k], onodes[k]), k
+        # the reference-facing tree object builds deferred and waits on ctree
+        ct = clustering.tree(p[:100_000], f[:100_000])
+        assert ct.ctree.size == 100_000 and ct._nodes_ready
+        nodes = _native.node_fields(ct.ctree)
+        onodes = O.OracleTree(p[:100_000], f[:100_000], 4).nodes()
+        for k in nodes:
+            assert np.array_equal(nodes[k], onodes[k]), k
+    finally:
+        _native.destroy(t)
+        _native.destroy(tq)
+        _native.destroy(t2)  # its copy may still be running
