@@ -606,49 +606,314 @@ __global__ void k_mark(int n_u, const int *__restrict__ pos_seg, Segs sg, LevelB
     }
 }
 
-__global__ void k_part_flags(int n_u, const int *__restrict__ pos_seg, Segs sg,
-                             const int *__restrict__ a, const unsigned char *__restrict__ side,
-                             unsigned long long *flags)
+// ---- Stable three-way partition of the three superkey orders, one level.
+// Within every splitting segment [l, r] (at least four points, median
+// position med = (l + r + 1) / 2), the points of each order d go, in their
+// order, to [l, med) when k_mark put them left of the median (side 0), to
+// (med, r] when right (side 1), the median point itself to med; positions
+// outside splitting segments stay.  The destination of a point is its
+// segment's start plus the number of same-side points before it in the
+// segment: a segmented prefix count, computed in three launches over tiles of
+// kPtTile positions that handle all three orders at once (per-tile counts, one
+// block scanning the tile counts, then the move), with no waiting between
+// blocks.  Counts inside a tile fit 16 bits: left | right << 16 in a word.
+constexpr int kPtThreads = 256;
+constexpr int kPtItems = 8;  // consecutive positions per thread
+constexpr int kPtTile = kPtThreads * kPtItems;
+
+struct PartIO {
+    const int *a[3];     // superkey orders (point ids by position)
+    int *ao[3];          // partitioned orders
+    const double *c[3];  // coordinate d of the point at each position of order d
+    double *co[3];       // the same, partitioned
+};
+
+// kPtItems consecutive ints from p + base (vector loads when all are in range)
+__device__ __forceinline__ void load8(const int *__restrict__ p, int base, int n, int (&x)[kPtItems])
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_u; i += gridDim.x * blockDim.x) {
-        int s = pos_seg[i];
-        unsigned long long f = 0;
-        if (s >= 0 && sg.r[s] - sg.l[s] + 1 >= 4) {
-            int sd = side[a[i]];
-            f = (sd == 0) ? 1ull : (sd == 1 ? (1ull << 32) : 0ull);
-        }
-        flags[i] = f;
+    static_assert(kPtItems == 8, "two int4 loads per thread");
+    if (base + kPtItems <= n) {
+        const int4 u = __ldg(reinterpret_cast<const int4 *>(p + base));
+        const int4 w = __ldg(reinterpret_cast<const int4 *>(p + base) + 1);
+        x[0] = u.x, x[1] = u.y, x[2] = u.z, x[3] = u.w;
+        x[4] = w.x, x[5] = w.y, x[6] = w.z, x[7] = w.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPtItems; k++) x[k] = base + k < n ? p[base + k] : -1;
     }
 }
 
-// moves index a[i] and its carried coordinate coord[i] to their
-// stable-partition position in out / coord_out
-__global__ void k_part_scatter(int n_u, const int *__restrict__ pos_seg, Segs sg,
-                               const int *__restrict__ a, const unsigned char *__restrict__ side,
-                               const unsigned long long *__restrict__ scan, int *out,
-                               const double *__restrict__ coord, double *coord_out, int *err)
+// the splitting segment of each of a thread's positions (-1: none) and the
+// positions that start one
+__device__ __forceinline__ unsigned split_segs(int base, int n_u, const int *__restrict__ pos_seg,
+                                               Segs sg, int (&sgi)[kPtItems])
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_u; i += gridDim.x * blockDim.x) {
-        int s = pos_seg[i];
-        int pt = a[i];
-        int dst = i;
-        if (s >= 0) {
-            int l = sg.l[s], r = sg.r[s];
-            if (r - l + 1 >= 4) {
-                int med = (l + r + 1) / 2;
-                int sd = side[pt];
-                unsigned long long c = scan[i], c0 = scan[l];
-                if (sd == 0) dst = l + (int)((uint32_t)c - (uint32_t)c0);
-                else if (sd == 1) dst = med + 1 + (int)((uint32_t)(c >> 32) - (uint32_t)(c0 >> 32));
-                else dst = med;
+    load8(pos_seg, base, n_u, sgi);
+    unsigned headmask = 0;
+#pragma unroll
+    for (int k = 0; k < kPtItems; k++) {
+        const int s = sgi[k];
+        if (s < 0) continue;
+        const int l = sg.l[s], r = sg.r[s];
+        if (r - l + 1 < 4) sgi[k] = -1;
+        else if (base + k == l) headmask |= 1u << k;
+    }
+    return headmask;
+}
+
+__device__ __forceinline__ unsigned side_count(int sd)
+{
+    return sd == 0 ? 1u : (sd == 1 ? 0x10000u : 0u);
+}
+
+// inclusive segmented scan over the lanes of a warp: a lane's value restarts
+// at a lane holding a head (f = 1)
+template <int NV>
+__device__ __forceinline__ void warp_seg_scan(unsigned &f, unsigned (&v)[NV], int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned pf = __shfl_up_sync(0xffffffffu, f, o);
+        unsigned pv[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++) pv[k] = __shfl_up_sync(0xffffffffu, v[k], o);
+        if (lane >= o) {
+            if (!f)
+#pragma unroll
+                for (int k = 0; k < NV; k++) v[k] += pv[k];
+            f |= pf;
+        }
+    }
+}
+
+// Per tile: (a head in the tile?, the three orders' packed side counts from
+// the tile's last head, or from its start when it has none).  Also stores
+// the three sides of every position, sd_pos[i] = side0 | side1 << 8 |
+// side2 << 16 (3: not in a splitting segment), so that the move reads them
+// in order instead of gathering side[] by point again.
+__global__ void __launch_bounds__(kPtThreads) k_part_count(int n_u, const int *__restrict__ pos_seg,
+                                                           Segs sg, const int *__restrict__ a0,
+                                                           const int *__restrict__ a1,
+                                                           const int *__restrict__ a2,
+                                                           const unsigned char *__restrict__ side,
+                                                           unsigned *sd_pos, uint4 *tagg)
+{
+    constexpr int NW = kPtThreads / 32;
+    __shared__ unsigned wf[NW], wv[NW][3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int base = blockIdx.x * kPtTile + threadIdx.x * kPtItems;
+    int sgi[kPtItems];
+    const unsigned headmask = split_segs(base, n_u, pos_seg, sg, sgi);
+    unsigned sdw[kPtItems];
+#pragma unroll
+    for (int k = 0; k < kPtItems; k++) sdw[k] = 0x030303u;
+    {
+        const int *ad[3] = {a0, a1, a2};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            int pt[kPtItems];
+            load8(ad[d], base, n_u, pt);
+#pragma unroll
+            for (int k = 0; k < kPtItems; k++)
+                if (sgi[k] >= 0)
+                    sdw[k] = (sdw[k] & ~(0xffu << (8 * d))) | ((unsigned)side[pt[k]] << (8 * d));
+        }
+    }
+    unsigned f = 0, v[3] = {0u, 0u, 0u};
+#pragma unroll
+    for (int k = 0; k < kPtItems; k++) {
+        if (headmask >> k & 1) {
+            f = 1;
+            v[0] = v[1] = v[2] = 0;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; d++) v[d] += side_count((sdw[k] >> (8 * d)) & 0xff);
+    }
+    if (base + kPtItems <= n_u) {
+        reinterpret_cast<uint4 *>(sd_pos + base)[0] = make_uint4(sdw[0], sdw[1], sdw[2], sdw[3]);
+        reinterpret_cast<uint4 *>(sd_pos + base)[1] = make_uint4(sdw[4], sdw[5], sdw[6], sdw[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPtItems; k++)
+            if (base + k < n_u) sd_pos[base + k] = sdw[k];
+    }
+    warp_seg_scan<3>(f, v, lane);
+    if (lane == 31) {
+        wf[w] = f;
+        wv[w][0] = v[0];
+        wv[w][1] = v[1];
+        wv[w][2] = v[2];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned F = 0, V[3] = {0u, 0u, 0u};
+        for (int q = 0; q < NW; q++) {
+            for (int k = 0; k < 3; k++) V[k] = wf[q] ? wv[q][k] : V[k] + wv[q][k];
+            F |= wf[q];
+        }
+        tagg[blockIdx.x] = make_uint4(F, V[0], V[1], V[2]);
+    }
+}
+
+
+__device__ __forceinline__ void unpack_counts(const uint4 &g, unsigned (&x)[6])
+{
+    x[0] = g.y & 0xffffu;
+    x[1] = g.y >> 16;
+    x[2] = g.z & 0xffffu;
+    x[3] = g.z >> 16;
+    x[4] = g.w & 0xffffu;
+    x[5] = g.w >> 16;
+}
+
+// One block: for every tile, the side counts (left, right for each order, 32
+// bits each) from the last head before the tile: carry[2t], carry[2t+1].
+__global__ void __launch_bounds__(1024) k_part_carry(int ntiles, const uint4 *__restrict__ tagg,
+                                                     uint4 *carry)
+{
+    __shared__ unsigned sf[32], sv[32][6];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int per = (ntiles + 1023) / 1024;
+    const int j0 = min(ntiles, t * per), j1 = min(ntiles, j0 + per);
+    unsigned f = 0, v[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+    for (int j = j0; j < j1; j++) {
+        const uint4 g = tagg[j];
+        unsigned x[6];
+        unpack_counts(g, x);
+        for (int k = 0; k < 6; k++) v[k] = g.x ? x[k] : v[k] + x[k];
+        f |= g.x;
+    }
+    unsigned fi = f, vi[6];
+    for (int k = 0; k < 6; k++) vi[k] = v[k];
+    warp_seg_scan<6>(fi, vi, lane);
+    if (lane == 31) {
+        sf[w] = fi;
+        for (int k = 0; k < 6; k++) sv[w][k] = vi[k];
+    }
+    __syncthreads();
+    // everything before this thread's tiles: the earlier warps, then the
+    // earlier lanes of this warp
+    unsigned pv[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+    for (int q = 0; q < w; q++)
+        for (int k = 0; k < 6; k++) pv[k] = sf[q] ? sv[q][k] : pv[k] + sv[q][k];
+    unsigned ef = __shfl_up_sync(0xffffffffu, fi, 1), ev[6];
+    for (int k = 0; k < 6; k++) ev[k] = __shfl_up_sync(0xffffffffu, vi[k], 1);
+    if (lane == 0) {
+        ef = 0;
+        for (int k = 0; k < 6; k++) ev[k] = 0;
+    }
+    unsigned cv[6];
+    for (int k = 0; k < 6; k++) cv[k] = ef ? ev[k] : pv[k] + ev[k];
+    for (int j = j0; j < j1; j++) {
+        carry[2 * (size_t)j] = make_uint4(cv[0], cv[1], cv[2], cv[3]);
+        carry[2 * (size_t)j + 1] = make_uint4(cv[4], cv[5], 0u, 0u);
+        const uint4 g = tagg[j];
+        unsigned x[6];
+        unpack_counts(g, x);
+        for (int k = 0; k < 6; k++) cv[k] = g.x ? x[k] : cv[k] + x[k];
+    }
+}
+
+// The move: every position's point id and carried coordinate, in each of the
+// three orders, to its place (see above).
+__global__ void __launch_bounds__(kPtThreads, 3) k_part_move(int n_u, const int *__restrict__ pos_seg,
+                                                             Segs sg, PartIO io,
+                                                             const unsigned *__restrict__ sd_pos,
+                                                             const uint4 *__restrict__ carry,
+                                                             int *err)
+{
+    constexpr int NW = kPtThreads / 32;
+    __shared__ unsigned wf[NW], wv[NW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int base = blockIdx.x * kPtTile + threadIdx.x * kPtItems;
+    const bool full = base + kPtItems <= n_u;
+    int sgi[kPtItems], sdp[kPtItems];
+    const unsigned headmask = split_segs(base, n_u, pos_seg, sg, sgi);
+    load8(reinterpret_cast<const int *>(sd_pos), base, n_u, sdp);
+    const uint4 c0 = carry[2 * (size_t)blockIdx.x], c1 = carry[2 * (size_t)blockIdx.x + 1];
+#pragma unroll 1
+    for (int d = 0; d < 3; d++) {
+        // (selects rather than indexing io and the carry by d, which would
+        // put them in local memory)
+        const int *__restrict__ ain = d == 0 ? io.a[0] : (d == 1 ? io.a[1] : io.a[2]);
+        int *__restrict__ aout = d == 0 ? io.ao[0] : (d == 1 ? io.ao[1] : io.ao[2]);
+        const double *__restrict__ cin = d == 0 ? io.c[0] : (d == 1 ? io.c[1] : io.c[2]);
+        double *__restrict__ cout = d == 0 ? io.co[0] : (d == 1 ? io.co[1] : io.co[2]);
+        const unsigned crl = d == 0 ? c0.x : (d == 1 ? c0.z : c1.x);
+        const unsigned crr = d == 0 ? c0.y : (d == 1 ? c0.w : c1.y);
+        int sd[kPtItems];
+        unsigned f = 0, v = 0;
+#pragma unroll
+        for (int k = 0; k < kPtItems; k++) {
+            sd[k] = ((unsigned)sdp[k] >> (8 * d)) & 0xffu;
+            if (headmask >> k & 1) {
+                f = 1;
+                v = 0;
+            }
+            v += side_count(sd[k]);
+        }
+        unsigned vi[1] = {v};
+        unsigned fi = f;
+        warp_seg_scan<1>(fi, vi, lane);
+        if (lane == 31) {
+            wf[w] = fi;
+            wv[w] = vi[0];
+        }
+        __syncthreads();
+        unsigned pf = 0, pv = 0;
+        for (int q = 0; q < w; q++) {
+            pv = wf[q] ? wv[q] : pv + wv[q];
+            pf |= wf[q];
+        }
+        unsigned ef = __shfl_up_sync(0xffffffffu, fi, 1);
+        unsigned ev = __shfl_up_sync(0xffffffffu, vi[0], 1);
+        if (lane == 0) ef = ev = 0;
+        // the tile's counts before this thread's first position
+        unsigned runf = pf | ef, runv = ef ? ev : pv + ev;
+        __syncthreads();  // wf / wv are written again for the next order
+        int pt[kPtItems];
+        double cv[kPtItems];
+        load8(ain, base, n_u, pt);
+        if (full) {
+            const double2 *cp = reinterpret_cast<const double2 *>(cin + base);
+#pragma unroll
+            for (int k = 0; k < kPtItems / 2; k++) {
+                const double2 t = __ldg(cp + k);
+                cv[2 * k] = t.x;
+                cv[2 * k + 1] = t.y;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kPtItems; k++) cv[k] = base + k < n_u ? cin[base + k] : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < kPtItems; k++) {
+            const int i = base + k;
+            if (i >= n_u) break;
+            int dst = i;
+            if (sgi[k] >= 0) {
+                if (headmask >> k & 1) {
+                    runf = 1;
+                    runv = 0;
+                }
+                unsigned L = runv & 0xffffu, R = runv >> 16;
+                if (!runf) {  // the segment began in an earlier tile
+                    L += crl;
+                    R += crr;
+                }
+                const int s = sgi[k], l = sg.l[s], r = sg.r[s], med = (l + r + 1) / 2;
+                dst = sd[k] == 0 ? l + (int)L : (sd[k] == 1 ? med + 1 + (int)R : med);
                 if (dst < l || dst > r) {
                     set_err(err, KD_EINTERNAL);
-                    continue;
+                    dst = -1;
                 }
+                runv += side_count(sd[k]);
+            }
+            if (dst >= 0) {
+                aout[dst] = pt[k];
+                cout[dst] = cv[k];
             }
         }
-        out[dst] = pt;
-        coord_out[dst] = coord[i];
     }
 }
 
@@ -1331,8 +1596,9 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     lb.haskids = pool.alloc<int>(cap);
     int *pos[2] = {pool.alloc<int>(n_u), pool.alloc<int>(n_u)};
     unsigned char *side = pool.alloc<unsigned char>(n_u);
-    unsigned long long *pf = pool.alloc<unsigned long long>(n_u),
-                       *ps = pool.alloc<unsigned long long>(n_u);
+    const int ntiles = (int)((n_u + (long long)kPtTile - 1) / kPtTile);
+    uint4 *tagg = pool.alloc<uint4>(ntiles), *tcarry = pool.alloc<uint4>(2 * (size_t)ntiles);
+    unsigned *sd_pos = pool.alloc<unsigned>(n_u);
     {
         int one = 1, zero = 0, last = n_u - 1;
         check(cudaMemcpyAsync(sg[0].count, &one, sizeof(int), cudaMemcpyHostToDevice, s), "H2D");
@@ -1409,6 +1675,16 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
         }
     }
 
+    // the partition kernels read and write these with 16-byte vector
+    // accesses at multiples of 8 elements: stream-ordered allocations are
+    // aligned far beyond that, which is checked here rather than assumed
+    {
+        const void *vec[] = {pos[0], pos[1], A[0], A[1], A[2], B[0], B[1], B[2],
+                             C[0],   C[1],   C[2], CB[0], CB[1], CB[2], sd_pos};
+        for (const void *p : vec)
+            if ((reinterpret_cast<uintptr_t>(p) & 15) != 0)
+                raise(KD_EINTERNAL, "build array not 16-byte aligned");
+    }
     int cur = 0, nlevels = 0;
     for (int lev = 0; (1LL << lev) <= (long long)n_u; lev++) {
         nlevels = lev + 1;
@@ -1435,13 +1711,22 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
             if (upto - node_queued >= ((size_t)4 << 20)) queue_nodes(upto);
         }
         k_mark<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, lb, A[0], A[1], A[2], side);
-        for (int d = 0; d < 3; d++) {
-            k_part_flags<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, A[d], side, pf);
-            excl_sum(pool, s, pf, ps, n_u);
-            k_part_scatter<<<grid_for(n_u), TPB, 0, s>>>(n_u, pos[cur], S, A[d], side, ps, B[d],
-                                                          C[d], CB[d], err);
-            std::swap(A[d], B[d]);
-            std::swap(C[d], CB[d]);
+        {
+            k_part_count<<<ntiles, kPtThreads, 0, s>>>(n_u, pos[cur], S, A[0], A[1], A[2], side,
+                                                       sd_pos, tagg);
+            k_part_carry<<<1, 1024, 0, s>>>(ntiles, tagg, tcarry);
+            PartIO io;
+            for (int d = 0; d < 3; d++) {
+                io.a[d] = A[d];
+                io.ao[d] = B[d];
+                io.c[d] = C[d];
+                io.co[d] = CB[d];
+            }
+            k_part_move<<<ntiles, kPtThreads, 0, s>>>(n_u, pos[cur], S, io, sd_pos, tcarry, err);
+            for (int d = 0; d < 3; d++) {
+                std::swap(A[d], B[d]);
+                std::swap(C[d], CB[d]);
+            }
         }
         excl_sum(pool, s, lb.haskids, lb.rank, ub);
         k_children<<<gs, TPB, 0, s>>>(S, ub, lb, N, cap, err);
