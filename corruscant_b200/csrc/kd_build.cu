@@ -2032,31 +2032,49 @@ struct Staging {
     void *pin[2] = {nullptr, nullptr};
 };
 // pinned staging pairs kept for the life of the process (allocating pinned
-// memory per copy costs more than the copy): one per copy running at once
+// memory per copy costs more than the copy): one per copy running at once,
+// at most kMaxStaging (a batch of many small deferred builds would otherwise
+// pin 64 MB per build); a copy that finds them all in use waits for one
+constexpr int kMaxStaging = 4;
 std::mutex g_stage_mu;
+std::condition_variable g_stage_cv;
 std::vector<Staging *> g_stage_free;
+int g_stage_made = 0;
 struct StagingLease {
     Staging *st = nullptr;
     StagingLease()
     {
         {
-            std::lock_guard<std::mutex> g(g_stage_mu);
+            std::unique_lock<std::mutex> g(g_stage_mu);
+            g_stage_cv.wait(g, [] { return !g_stage_free.empty() || g_stage_made < kMaxStaging; });
             if (!g_stage_free.empty()) {
                 st = g_stage_free.back();
                 g_stage_free.pop_back();
                 return;
             }
+            g_stage_made++;  // this thread makes the next pair
         }
         std::unique_ptr<Staging> n(new Staging);
         for (int i = 0; i < 2; i++)
-            check(cudaHostAlloc(&n->pin[i], Staging::kChunk, cudaHostAllocPortable),
-                  "cudaHostAlloc");
+            if (cudaHostAlloc(&n->pin[i], Staging::kChunk, cudaHostAllocPortable) != cudaSuccess) {
+                cudaGetLastError();
+                for (int j = 0; j < i; j++) cudaFreeHost(n->pin[j]);
+                {
+                    std::lock_guard<std::mutex> g(g_stage_mu);
+                    g_stage_made--;
+                }
+                g_stage_cv.notify_one();
+                raise(KD_ENOMEM, "out of pinned host memory for the node array copy");
+            }
         st = n.release();
     }
     ~StagingLease()
     {
-        std::lock_guard<std::mutex> g(g_stage_mu);
-        g_stage_free.push_back(st);
+        {
+            std::lock_guard<std::mutex> g(g_stage_mu);
+            g_stage_free.push_back(st);
+        }
+        g_stage_cv.notify_one();
     }
 };
 }  // namespace
