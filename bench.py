@@ -32,13 +32,13 @@ A step is every count of the workload for all edges: one kd_count_batch call
 on prebuilt trees, inputs resident in HBM.  value = pairs tested per second,
 all ranks, with the mixed FP32 + FP64-recheck counter; the plain FP64 counter
 is timed on the same steps.  e2e = a full result end to end through the C ABI
-from pinned host buffers: kd_tree_construct_deferred of every catalog, one
-after the other (H2D of the points; for the angular workload the RA/DEC
-conversion too), the batched count while the node arrays drain to the host, results
-read back and every node array complete on the host (kd_tree_wait_nodes),
-every step; its value is in
-all-pairs-equivalent pairs per second (sum of Nq * Nt over the counts per
-second of a full result), the unit the reference arm's e2e uses too, so that
+from pinned host buffers, every step: kd_tree_construct_deferred of every
+catalog (one after the other; four at a time for the 129 mock catalogs),
+with the H2D of the points and, for the angular workload, the RA/DEC
+conversion; the batched count while the node arrays drain to the host; the
+results read back and every node array complete on the host
+(kd_tree_wait_nodes).  Its value is in all-pairs-equivalent pairs per
+second (sum of Nq * Nt over the counts per second of a full result), the unit the reference arm's e2e uses too, so that
 their ratio is the ratio of times per full result.  Also reported: the FP64
 form against its CUDA-core peak, the time per full result and an FP32-pipe
 model of the binning (FMA lane-ops per pair from the measured active edges
@@ -76,7 +76,11 @@ UNIT = "pairs/s"
 # end-to-end rates of both arms: exhaustive-equivalent pairs (sum of Nq * Nt
 # over the counts) per second of a full result, comparable across algorithms
 E2E_UNIT = "all-pairs-equivalent pairs/s"
-E2E_BUILD_WORKERS = 1  # catalogs built at once in the end-to-end steps (2 measured slower)
+# catalogs built at once in the end-to-end steps: one after the other for a
+# few large catalogs (two at once measured slower on the clustered workload),
+# four at once for many small ones (the 129 mock catalogs: 0.28 s against
+# 0.62 s one after the other)
+E2E_BUILD_WORKERS_FEW, E2E_BUILD_WORKERS_MANY = 1, 4
 FLOP_PER_PAIR = 8  # 3 subtractions, 1 multiply, 2 fused multiply-adds per distance
 
 # ---------------------------------------------------------------- workloads
@@ -422,6 +426,10 @@ def _build_all(N, w, convert=False, host=None, deferred=False, workers=1):
         return dict(ex.map(one, items))
 
 
+def _e2e_workers(w):
+    return E2E_BUILD_WORKERS_MANY if len(w.catalogs) > 4 else E2E_BUILD_WORKERS_FEW
+
+
 def _pinned_copies(w):
     """Page-locked copies of every input array (points, fields, RA/DEC), the
     host buffers the end-to-end steps copy to the device from.  The torch
@@ -525,7 +533,7 @@ def _measure(N, D, w, steps, warmup):
     for it in range(1 + steps):
         D.barrier()
         t0 = time.perf_counter()
-        tt = _build_all(N, w, convert=True, host=host, deferred=True, workers=E2E_BUILD_WORKERS)
+        tt = _build_all(N, w, convert=True, host=host, deferred=True, workers=_e2e_workers(w))
         _, s = N.count_batch([(tt[t], tt[q]) for _, t, q in w.jobs], radii, with_stats=True,
                              shard=D.rank, nshards=D.world)
         for t in tt.values():  # every node array complete on the host
@@ -639,7 +647,7 @@ def _summary(w, m, steps, peak, peak64, D):
                 "s_per_step": e_s, "s_per_full_result": e_s,
                 "pairs_tested_per_s": m["e_pairs"] / m["e_wall"],
                 "host_buffers": "pinned" if m["pinned"] else "pageable",
-                "builds": (f"kd_tree_construct_deferred, {E2E_BUILD_WORKERS} catalogs at a time; "
+                "builds": (f"kd_tree_construct_deferred, {_e2e_workers(w)} catalog(s) at a time; "
                            "node arrays complete on the host before the step ends"),
                 "count_device_s_last_step": m["e2e_count_s"],
                 "build_stats_last_step": m["build_stats"]},

@@ -89,43 +89,6 @@ void init_device()
     done.fetch_or(bit);
 }
 
-// The device pool of the node arrays that builds copy to the host.  It is
-// kept apart from the default pool that every other build and count array
-// comes from: a node array still being copied while a count runs (deferred
-// builds) would otherwise sit inside a cached block of the default pool that
-// the count's large tile-record buffer could have reused, and the pool would
-// grow (new physical memory) for that buffer instead.
-static cudaMemPool_t node_pool()
-{
-    static std::mutex mu;
-    static cudaMemPool_t pools[64] = {};
-    int dev = 0;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    cudaMemPool_t def = nullptr;
-    if (dev < 0 || dev >= 64) {
-        check(cudaDeviceGetDefaultMemPool(&def, dev), "cudaDeviceGetDefaultMemPool");
-        return def;
-    }
-    std::lock_guard<std::mutex> g(mu);
-    if (!pools[dev]) {
-        cudaMemPoolProps props;
-        memset(&props, 0, sizeof props);
-        props.allocType = cudaMemAllocationTypePinned;
-        props.location.type = cudaMemLocationTypeDevice;
-        props.location.id = dev;
-        cudaMemPool_t p = nullptr;
-        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
-            cudaGetLastError();  // no pool of its own: the default one serves
-            check(cudaDeviceGetDefaultMemPool(&def, dev), "cudaDeviceGetDefaultMemPool");
-            return def;
-        }
-        uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &thr);
-        pools[dev] = p;
-    }
-    return pools[dev];
-}
-
 // Order-preserving 64-bit key of a double; -0.0 maps to +0.0's key so that
 // key equality is C '==' equality for non-NaN values.
 __device__ __forceinline__ uint64_t okey(double v)
@@ -1570,7 +1533,7 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
     }
     TreeOut to;
     to.memsize = memsize;
-    to.nodes = sink ? keep.alloc_from<NodeRec>(node_pool(), memsize) : keep.alloc<NodeRec>(memsize);
+    to.nodes = sink ? keep.alloc_from<NodeRec>(side_pool(kPoolNodes), memsize) : keep.alloc<NodeRec>(memsize);
     to.npoint = pool.alloc<int>(memsize);
     to.ndim = pool.alloc<unsigned char>(memsize);
     to.inorder_u = pool.alloc<int>(n_u);

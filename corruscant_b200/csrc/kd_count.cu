@@ -1102,8 +1102,18 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
         total += hcnt[i];
         maxblk = std::max<long long>(maxblk, hcnt[i]);
     }
+    // free memory: the driver's, plus what the record pool and the default
+    // pool hold cached (reusable without asking the driver)
+    const cudaMemPool_t rpool = side_pool(kPoolRecords);
     size_t freeb = 0, totb = 0;
     cudaMemGetInfo(&freeb, &totb);
+    freeb += pool_idle_bytes(rpool);
+    {
+        cudaMemPool_t dpool = nullptr;
+        if (cudaDeviceGetDefaultMemPool(&dpool, device) == cudaSuccess && dpool != rpool)
+            freeb += pool_idle_bytes(dpool);
+        cudaGetLastError();
+    }
     long long cap = std::max<long long>(
         1 << 20, std::min<long long>(1LL << 30, (long long)(freeb / 4 / sizeof(uint4))));
     // KD_TILE_RECORD_CAP (records, > 0) lowers the batch size: it exercises
@@ -1116,7 +1126,7 @@ static void count_batch_impl(const kd_catalog *const *tcs, const kd_catalog *con
     // largest block's records (a failed allocation is reported, not overrun)
     cap = std::max(cap, maxblk);
     cap = std::min<long long>(cap, std::max<long long>(total, 1));
-    uint4 *rec = pool.alloc<uint4>(cap);
+    uint4 *rec = pool.alloc_from<uint4>(rpool, cap);
     long long *off = pool.alloc<long long>(nb + 1);
     std::vector<long long> hoffs(nb + 1);
 
