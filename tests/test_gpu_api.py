@@ -134,3 +134,35 @@ def test_deferred_build_counts_while_node_array_drains():
         _native.destroy(t)
         _native.destroy(tq)
         _native.destroy(t2)  # its copy may still be running
+
+
+def test_many_deferred_builds_share_four_staging_pairs():
+    """Twelve deferred builds whose node arrays (each above 4 MB) drain at
+    once: at most four copies hold a pinned staging pair, the others wait
+    for one; every node array arrives complete, from builds on one thread
+    and on four threads at once."""
+    from concurrent.futures import ThreadPoolExecutor
+    rs = np.random.RandomState(10)
+    cats = [rs.rand(int(n), 3) for n in rs.randint(150_000, 400_000, 12)]
+    fields = [(c[:, 2] * 3).astype(np.int32) for c in cats]
+    want = [O.OracleTree(c, f, 3).nodes() for c, f in zip(cats[:3], fields[:3])]
+    for workers in (1, 4):
+        def one(i):
+            return _native.build_tree(cats[i], fields[i], 3, deferred=True)
+        if workers == 1:
+            trees = [one(i) for i in range(12)]
+        else:
+            with ThreadPoolExecutor(max_workers=workers) as ex:
+                trees = list(ex.map(one, range(12)))
+        try:
+            for t in trees:
+                _native.wait_nodes(t)
+            for t, c, wn in zip(trees, cats, want):
+                got = _native.node_fields(t)
+                for k in got:
+                    assert np.array_equal(got[k], wn[k]), k
+            for t, c in zip(trees, cats):
+                assert t.size == len(c)
+        finally:
+            for t in trees:
+                _native.destroy(t)
