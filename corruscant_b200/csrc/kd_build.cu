@@ -1321,6 +1321,7 @@ template <class T> static T read1(const T *d, cudaStream_t s)
 }
 
 static void copy_to_pageable(void *dst, const void *src, size_t bytes);
+static void copy_from_host(void *dst, const void *src, size_t bytes, cudaStream_t s);
 
 // Touch one byte of every 4 KiB page of [p, p + bytes), split over up to 16
 // threads, so that the pages are resident before they are copied into.
@@ -1421,13 +1422,11 @@ static void build_impl(const double *h_xyz, const int *h_fields, int n, int num_
 
     // ---- inputs
     double *xyz = pool.alloc<double>(3 * (size_t)n);
-    check(cudaMemcpyAsync(xyz, h_xyz, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, s),
-          "H2D points");
+    copy_from_host(xyz, h_xyz, sizeof(double) * 3 * (size_t)n, s);
     int *fin = nullptr;
     if (h_fields) {
         fin = pool.alloc<int>(n);
-        check(cudaMemcpyAsync(fin, h_fields, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s),
-              "H2D fields");
+        copy_from_host(fin, h_fields, sizeof(int) * (size_t)n, s);
     }
     int *err = pool.alloc<int>(1);
     unsigned long long *misc = pool.alloc<unsigned long long>(4);
@@ -2040,7 +2039,132 @@ struct StagingLease {
         g_stage_cv.notify_one();
     }
 };
+// Host copies of a transfer's chunks fanned out over a pool of threads made
+// once for the whole transfer (a 32 MB chunk takes ~1 ms; creating threads
+// per chunk would cost a good part of that).  Transfers under 4 MB are
+// copied by the calling thread alone.
+struct FanOut {
+    int nthr = 1;
+    std::vector<std::thread> th;
+    std::mutex mu;
+    std::condition_variable go, done;
+    size_t gen = 0;
+    int pending = 0;
+    bool stop = false;
+    char *to = nullptr;
+    const char *from = nullptr;
+    size_t len = 0;
+    explicit FanOut(size_t bytes)
+    {
+        const unsigned hw = std::thread::hardware_concurrency();
+        nthr = bytes < (size_t(4) << 20) ? 1 : (int)std::max(1u, std::min(16u, hw ? hw : 1u));
+        try {
+            for (int t = 1; t < nthr; t++) th.emplace_back(&FanOut::worker, this, t);
+        } catch (const std::exception &) {  // fewer threads: the rest is copied by this one
+        }
+    }
+    void slice(int t, char *d, const char *f, size_t n)
+    {
+        const size_t a = n * t / nthr, b = n * (t + 1) / nthr;
+        std::memcpy(d + a, f + a, b - a);
+    }
+    void worker(int t)
+    {
+        size_t seen = 0;
+        std::unique_lock<std::mutex> g(mu);
+        for (;;) {
+            go.wait(g, [&] { return stop || gen != seen; });
+            if (stop) return;
+            seen = gen;
+            char *d = to;
+            const char *f = from;
+            const size_t n = len;
+            g.unlock();
+            slice(t, d, f, n);
+            g.lock();
+            if (--pending == 0) done.notify_one();
+        }
+    }
+    void copy(char *d, const char *f, size_t n)
+    {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            to = d;
+            from = f;
+            len = n;
+            pending = (int)th.size();
+            gen++;
+        }
+        go.notify_all();
+        // slices of the threads that could not be started are done here
+        for (int t = (int)th.size() + 1; t < nthr; t++) slice(t, d, f, n);
+        slice(0, d, f, n);
+        std::unique_lock<std::mutex> g(mu);
+        done.wait(g, [&] { return pending == 0; });
+    }
+    ~FanOut()
+    {
+        {
+            std::lock_guard<std::mutex> g(mu);
+            stop = true;
+        }
+        go.notify_all();
+        for (auto &x : th) x.join();
+    }
+};
 }  // namespace
+
+// Host -> device copy of a build's input on stream s.  Pinned (or managed)
+// memory, and anything under 32 MB (where starting the copying threads
+// costs more than it saves), is one cudaMemcpyAsync.  Pageable memory
+// otherwise takes the driver's own staging path at about 10 GB/s (50 ms for
+// the 560 MB of a 20M-point catalog); here several threads copy each 32 MB
+// chunk into a pinned staging buffer while the previous chunk's DMA runs.
+// Returns once the last DMA has finished (the staging pair is then free).
+static void copy_from_host(void *dst, const void *src, size_t bytes, cudaStream_t s)
+{
+    if (bytes == 0) return;
+    bool plain = bytes < (size_t(32) << 20);
+    if (!plain) {
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, src) == cudaSuccess)
+            plain = at.type != cudaMemoryTypeUnregistered;
+        else
+            cudaGetLastError();  // not known to the runtime: pageable
+    }
+    if (plain) {
+        check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "H2D");
+        return;
+    }
+    const size_t chunk = Staging::kChunk;
+    StagingLease lease;
+    void *const *pin = lease.st->pin;
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    struct Release {
+        cudaEvent_t *ev;
+        ~Release()
+        {
+            for (int i = 0; i < 2; i++)
+                if (ev[i]) {
+                    cudaEventSynchronize(ev[i]);  // no DMA may still read the staging
+                    cudaEventDestroy(ev[i]);
+                }
+        }
+    } rel{done};
+    for (int i = 0; i < 2; i++)
+        check(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
+    FanOut fan(bytes);
+    const size_t nch = (bytes + chunk - 1) / chunk;
+    for (size_t c = 0; c < nch; c++) {
+        const int b = (int)(c & 1);
+        if (c >= 2) check(cudaEventSynchronize(done[b]), "H2D wait");  // its last DMA is done
+        const size_t off = c * chunk, len = std::min(chunk, bytes - off);
+        fan.copy((char *)pin[b], (const char *)src + off, len);
+        check(cudaMemcpyAsync((char *)dst + off, pin[b], len, cudaMemcpyHostToDevice, s), "H2D");
+        check(cudaEventRecord(done[b], s), "event");
+    }
+    for (int b = 0; b < 2; b++) check(cudaEventSynchronize(done[b]), "H2D wait");
+}
 
 static void copy_to_pageable(void *dst, const void *src, size_t bytes)
 {
@@ -2067,78 +2191,8 @@ static void copy_to_pageable(void *dst, const void *src, size_t bytes)
               "D2H");
         check(cudaEventRecord(done[c & 1], st.s), "event");
     };
-    // host copies of each chunk fanned out over a pool of threads made once
-    // for the whole call (a chunk takes ~1 ms; creating threads per chunk
-    // would cost a good part of that)
-    struct FanOut {
-        int nthr = 1;
-        std::vector<std::thread> th;
-        std::mutex mu;
-        std::condition_variable go, done;
-        size_t gen = 0;
-        int pending = 0;
-        bool stop = false;
-        char *to = nullptr;
-        const char *from = nullptr;
-        size_t len = 0;
-        void slice(int t, char *d, const char *f, size_t n)
-        {
-            const size_t a = n * t / nthr, b = n * (t + 1) / nthr;
-            std::memcpy(d + a, f + a, b - a);
-        }
-        void worker(int t)
-        {
-            size_t seen = 0;
-            std::unique_lock<std::mutex> g(mu);
-            for (;;) {
-                go.wait(g, [&] { return stop || gen != seen; });
-                if (stop) return;
-                seen = gen;
-                char *d = to;
-                const char *f = from;
-                const size_t n = len;
-                g.unlock();
-                slice(t, d, f, n);
-                g.lock();
-                if (--pending == 0) done.notify_one();
-            }
-        }
-        void copy(char *d, const char *f, size_t n)
-        {
-            {
-                std::lock_guard<std::mutex> g(mu);
-                to = d;
-                from = f;
-                len = n;
-                pending = (int)th.size();
-                gen++;
-            }
-            go.notify_all();
-            // slices of the threads that could not be started are done here
-            for (int t = (int)th.size() + 1; t < nthr; t++) slice(t, d, f, n);
-            slice(0, d, f, n);
-            std::unique_lock<std::mutex> g(mu);
-            done.wait(g, [&] { return pending == 0; });
-        }
-        ~FanOut()
-        {
-            {
-                std::lock_guard<std::mutex> g(mu);
-                stop = true;
-            }
-            go.notify_all();
-            for (auto &x : th) x.join();
-        }
-    } fan;
-    {
-        // small items (the top levels) are copied by this thread alone
-        const unsigned hw = std::thread::hardware_concurrency();
-        fan.nthr = bytes < (size_t(4) << 20) ? 1 : (int)std::max(1u, std::min(16u, hw ? hw : 1u));
-        try {
-            for (int t = 1; t < fan.nthr; t++) fan.th.emplace_back(&FanOut::worker, &fan, t);
-        } catch (const std::exception &) {  // fewer threads: the rest is copied by this one
-        }
-    }
+    FanOut fan(bytes);
+
     issue(0);
     for (size_t c = 0; c < nch; c++) {
         check(cudaEventSynchronize(done[c & 1]), "D2H wait");
