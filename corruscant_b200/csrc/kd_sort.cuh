@@ -199,19 +199,31 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_count(const K *keys, lon
         counts[(long long)d * ntiles + blockIdx.x] = h[d];
 }
 
-// stable scatter of one tile to offsets[d * ntiles + tile] + rank
+// Stable scatter of one tile to offsets[d * ntiles + tile] + rank.  The
+// tile is first ordered by digit in shared memory (ranks from per-warp digit
+// counts and warp matching of equal digits, as the tile's keys come: warp,
+// then round, then lane), then written out in that order, so that each
+// thread's consecutive stores of one digit land on consecutive addresses
+// (runs of ~8 keys per digit per tile at 256 digits) instead of 32 scattered
+// addresses per store instruction.
 template <class K, class V>
 __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const K *kin, K *kout, const V *vin,
                                                                 V *vout, long long n, int shift,
                                                                 int mask, const unsigned *offsets,
                                                                 long long ntiles)
 {
-    __shared__ unsigned wc[kSortWarps][kBins];  // per-warp counts, then running positions
+    __shared__ unsigned wc[kSortWarps][kBins];  // per-warp counts, then tile-local positions
+    __shared__ unsigned tstart[kBins];          // first tile-local position of each digit
+    __shared__ unsigned gofs[kBins];            // first output position of each digit
+    __shared__ unsigned wsum[kSortWarps];
+    __shared__ K skey[kSortTile];
+    __shared__ V sval[kSortTile];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kSortWarps * kBins; i += blockDim.x) (&wc[0][0])[i] = 0;
     __syncthreads();
     // warp w owns keys [w * 32 * kSortRounds, (w + 1) * 32 * kSortRounds) of the tile
-    const long long base = (long long)blockIdx.x * kSortTile + (long long)w * 32 * kSortRounds;
+    const long long tbase = (long long)blockIdx.x * kSortTile;
+    const long long base = tbase + (long long)w * 32 * kSortRounds;
     int dg[kSortRounds];
 #pragma unroll
     for (int r = 0; r < kSortRounds; r++) {
@@ -226,9 +238,28 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const K *kin, K 
         __syncwarp();
     }
     __syncthreads();
-    // positions: tile offset of the digit + counts of the earlier warps
-    for (int d = threadIdx.x; d <= mask; d += blockDim.x) {
-        unsigned run = offsets[(long long)d * ntiles + blockIdx.x];
+    // digit totals of the tile, their exclusive scan (one digit per thread),
+    // and each warp's first position within its digit
+    static_assert(kBins == kSortThreads, "one digit per thread");
+    {
+        const int d = threadIdx.x;
+        unsigned tot = 0;
+#pragma unroll
+        for (int k = 0; k < kSortWarps; k++) tot += wc[k][d];
+        unsigned inc = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        if (lane == 31) wsum[w] = inc;
+        __syncthreads();
+        unsigned before = 0;
+        for (int k = 0; k < w; k++) before += wsum[k];
+        unsigned run = before + inc - tot;
+        tstart[d] = run;
+        gofs[d] = d <= mask ? offsets[(long long)d * ntiles + blockIdx.x] : 0u;
+#pragma unroll
         for (int k = 0; k < kSortWarps; k++) {
             const unsigned c = wc[k][d];
             wc[k][d] = run;
@@ -236,6 +267,7 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const K *kin, K 
         }
     }
     __syncthreads();
+    // the tile in digit order, in shared memory
 #pragma unroll
     for (int r = 0; r < kSortRounds; r++) {
         const long long j = base + r * 32 + lane;
@@ -244,12 +276,24 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_scatter(const K *kin, K 
         if (v) {
             const unsigned peers = __match_any_sync(act, dg[r]);
             const unsigned pos = wc[w][dg[r]] + __popc(peers & ((1u << lane) - 1u));
-            kout[pos] = kin[j];
-            vout[pos] = vin[j];
+            skey[pos] = kin[j];
+            sval[pos] = vin[j];
             __syncwarp(act);
             if (lane == __ffs(peers) - 1) wc[w][dg[r]] += __popc(peers);
         }
         __syncwarp();
+    }
+    __syncthreads();
+    // written out in that order: consecutive positions of a digit go to
+    // consecutive output addresses
+    const long long left = n - tbase;
+    const int cnt = left < kSortTile ? (int)left : kSortTile;
+    for (int i = threadIdx.x; i < cnt; i += kSortThreads) {
+        const K k = skey[i];
+        const int d = digit_of(k, shift, mask);
+        const unsigned dst = gofs[d] + ((unsigned)i - tstart[d]);
+        kout[dst] = k;
+        vout[dst] = sval[i];
     }
 }
 
