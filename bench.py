@@ -671,7 +671,7 @@ def _config(w, world):
     return cfg
 
 
-# the other BASELINE workloads measured by the default run after the headline
+# the other workloads, measured by the default run after the headline one
 OTHER_WORKLOADS = ("angular", "mocks", "lattice")
 OTHER_STEPS = 3
 
