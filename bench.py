@@ -38,8 +38,9 @@ with the H2D of the points and, for the angular workload, the RA/DEC
 conversion; the batched count while the node arrays drain to the host; the
 results read back and every node array complete on the host
 (kd_tree_wait_nodes).  Its value is in all-pairs-equivalent pairs per
-second (sum of Nq * Nt over the counts per second of a full result), the unit the reference arm's e2e uses too, so that
-their ratio is the ratio of times per full result.  Also reported: the FP64
+second (sum of Nq * Nt over the counts per second of a full result), the
+unit the reference arm's e2e uses too, so that their ratio is the ratio of
+times per full result.  Also reported: the FP64
 form against its CUDA-core peak, the time per full result and an FP32-pipe
 model of the binning (FMA lane-ops per pair from the measured active edges
 per pair).  The default run then measures the angular, mocks and lattice
