@@ -166,3 +166,30 @@ def test_many_deferred_builds_share_four_staging_pairs():
         finally:
             for t in trees:
                 _native.destroy(t)
+
+
+def test_pinned_and_pageable_inputs_build_the_same_tree():
+    """A catalog's points above 32 MB go to the device through pinned staging
+    when they are pageable and in one copy when they are pinned: the same
+    tree either way, and the oracle's."""
+    torch = pytest.importorskip("torch")
+    rs = np.random.RandomState(12)
+    n = 2_000_000  # 48 MB of points
+    p = rs.rand(n, 3)
+    f = (p[:, 0] * 4).astype(np.int32)
+    pin = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    pin.numpy()[...] = p
+    pinf = torch.empty(n, dtype=torch.int32).pin_memory()
+    pinf.numpy()[...] = f
+    a = _native.build_tree(p, f, 4)
+    b = _native.build_tree(pin.numpy(), pinf.numpy(), 4)
+    try:
+        na, nb = _native.node_fields(a), _native.node_fields(b)
+        onodes = O.OracleTree(p, f, 4).nodes()
+        for k in na:
+            assert np.array_equal(na[k], nb[k]), k
+            assert np.array_equal(na[k], onodes[k]), k
+        assert np.array_equal(_native.permutation(a), _native.permutation(b))
+    finally:
+        _native.destroy(a)
+        _native.destroy(b)
