@@ -33,7 +33,8 @@ on prebuilt trees, inputs resident in HBM.  value = pairs tested per second,
 all ranks, with the mixed FP32 + FP64-recheck counter; the plain FP64 counter
 is timed on the same steps.  e2e = a full result end to end through the C ABI
 from pinned host buffers, every step: kd_tree_construct_deferred of every
-catalog (one after the other; four at a time for the 129 mock catalogs),
+catalog (one after the other; two at a time for the sky catalogs, four for
+the 129 mock catalogs),
 with the H2D of the points and, for the angular workload, the RA/DEC
 conversion; the batched count while the node arrays drain to the host; the
 results read back and every node array complete on the host
@@ -79,9 +80,10 @@ UNIT = "pairs/s"
 E2E_UNIT = "all-pairs-equivalent pairs/s"
 # catalogs built at once in the end-to-end steps: one after the other for a
 # few large catalogs (two at once measured slower on the clustered workload),
-# four at once for many small ones (the 129 mock catalogs: 0.28 s against
-# 0.62 s one after the other)
-E2E_BUILD_WORKERS_FEW, E2E_BUILD_WORKERS_MANY = 1, 4
+# two at once for sky catalogs, whose host RA/DEC conversion then overlaps the
+# other catalog's build (angular step 0.37 s against 0.39 s), four at once for
+# many small ones (the 129 mock catalogs: 0.28 s against 0.62 s of builds)
+E2E_BUILD_WORKERS_FEW, E2E_BUILD_WORKERS_SKY, E2E_BUILD_WORKERS_MANY = 1, 2, 4
 FLOP_PER_PAIR = 8  # 3 subtractions, 1 multiply, 2 fused multiply-adds per distance
 
 # ---------------------------------------------------------------- workloads
@@ -428,7 +430,9 @@ def _build_all(N, w, convert=False, host=None, deferred=False, workers=1):
 
 
 def _e2e_workers(w):
-    return E2E_BUILD_WORKERS_MANY if len(w.catalogs) > 4 else E2E_BUILD_WORKERS_FEW
+    if len(w.catalogs) > 4:
+        return E2E_BUILD_WORKERS_MANY
+    return E2E_BUILD_WORKERS_SKY if w.radec else E2E_BUILD_WORKERS_FEW
 
 
 def _pinned_copies(w):
