@@ -33,15 +33,13 @@ on prebuilt trees, inputs resident in HBM.  value = pairs tested per second,
 all ranks, with the mixed FP32 + FP64-recheck counter; the plain FP64 counter
 is timed on the same steps.  e2e = a full result end to end through the C ABI
 from pinned host buffers, every step: kd_tree_construct_deferred of every
-catalog (one after the other; two at a time for the sky catalogs, four for
-the 129 mock catalogs),
-with the H2D of the points and, for the angular workload, the RA/DEC
-conversion; the batched count while the node arrays drain to the host; the
-results read back and every node array complete on the host
-(kd_tree_wait_nodes).  Its value is in all-pairs-equivalent pairs per
-second (sum of Nq * Nt over the counts per second of a full result), the
-unit the reference arm's e2e uses too, so that their ratio is the ratio of
-times per full result.  Also reported: the FP64
+catalog (two at a time; four for the 129 mock catalogs), with the H2D of the
+points and, for the angular workload, the RA/DEC conversion; the batched
+count while the node arrays drain to the host; the results read back and
+every node array complete on the host (kd_tree_wait_nodes).  Its value is in
+all-pairs-equivalent pairs per second (sum of Nq * Nt over the counts per
+second of a full result), the unit the reference arm's e2e uses too, so that
+their ratio is the ratio of times per full result.  Also reported: the FP64
 form against its CUDA-core peak, the time per full result and an FP32-pipe
 model of the binning (FMA lane-ops per pair from the measured active edges
 per pair).  The default run then measures the angular, mocks and lattice
@@ -78,12 +76,12 @@ UNIT = "pairs/s"
 # end-to-end rates of both arms: exhaustive-equivalent pairs (sum of Nq * Nt
 # over the counts) per second of a full result, comparable across algorithms
 E2E_UNIT = "all-pairs-equivalent pairs/s"
-# catalogs built at once in the end-to-end steps: one after the other for a
-# few large catalogs (two at once measured slower on the clustered workload),
-# two at once for sky catalogs, whose host RA/DEC conversion then overlaps the
-# other catalog's build (angular step 0.37 s against 0.39 s), four at once for
-# many small ones (the 129 mock catalogs: 0.28 s against 0.62 s of builds)
-E2E_BUILD_WORKERS_FEW, E2E_BUILD_WORKERS_SKY, E2E_BUILD_WORKERS_MANY = 1, 2, 4
+# catalogs built at once in the end-to-end steps: two for a few large ones
+# (the smaller build, and for sky catalogs the host RA/DEC conversion, overlap
+# the larger: clustered builds 81 ms against 87 ms one after the other,
+# angular step 0.37 s against 0.39 s), four for many small ones (the 129 mock
+# catalogs: 0.28 s against 0.62 s of builds)
+E2E_BUILD_WORKERS_FEW, E2E_BUILD_WORKERS_MANY = 2, 4
 FLOP_PER_PAIR = 8  # 3 subtractions, 1 multiply, 2 fused multiply-adds per distance
 
 # ---------------------------------------------------------------- workloads
@@ -430,9 +428,7 @@ def _build_all(N, w, convert=False, host=None, deferred=False, workers=1):
 
 
 def _e2e_workers(w):
-    if len(w.catalogs) > 4:
-        return E2E_BUILD_WORKERS_MANY
-    return E2E_BUILD_WORKERS_SKY if w.radec else E2E_BUILD_WORKERS_FEW
+    return E2E_BUILD_WORKERS_MANY if len(w.catalogs) > 4 else E2E_BUILD_WORKERS_FEW
 
 
 def _pinned_copies(w):
