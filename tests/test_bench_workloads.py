@@ -42,3 +42,35 @@ def test_reference_leg_runs(name, scale):
     assert cb["kind"] == "reference" and cb["value"] > 0 and cb["pairs_tested_per_sample"] > 0
     if name == "angular":
         assert cb["coordinates_bit_identical"]
+
+
+class _FakeNative:
+    """Stands in for corruscant_b200._native in bench._build_all: records the
+    arguments of every build (from several threads at once)."""
+
+    def __init__(self):
+        import threading
+        self.lock = threading.Lock()
+        self.calls = []
+
+    def build_tree(self, pts, f, nf, deferred=False):
+        with self.lock:
+            self.calls.append((len(pts), nf, deferred))
+        return ("tree", len(pts))
+
+
+@pytest.mark.parametrize("name,workers", [("clustered3d", 2), ("mocks", 4), ("angular", 2)])
+def test_e2e_builds_every_catalog_once(name, workers):
+    w = bench.WORKLOADS[name](0.01 if name != "mocks" else 0.02)
+    assert bench._e2e_workers(w) == workers
+    fake = _FakeNative()
+    trees = bench._build_all(fake, w, convert=True, deferred=True, workers=workers)
+    assert sorted(trees) == sorted(w.catalogs)
+    assert len(fake.calls) == len(w.catalogs) and all(d for _, _, d in fake.calls)
+    for name_, (pts, f, nf) in w.catalogs.items():
+        assert trees[name_] == ("tree", len(pts))
+    # one at a time, the largest catalog is built first
+    fake1 = _FakeNative()
+    bench._build_all(fake1, w, convert=True, deferred=True, workers=1)
+    sizes = [n for n, _, _ in fake1.calls]
+    assert sizes == sorted(sizes, reverse=True)
